@@ -1,0 +1,441 @@
+#!/usr/bin/env python
+"""Headline benchmark: the P3BCA Simulation step on one B200 (C3: N=131072 uniform particles at
+density 2.048 in a 40^3 box, cutoff 2, mass 1, zero velocity, dt 0.001, g = (0,-9.81,0)), mixed
+precision, with the FP64 drop-in measured beside it.  Metric: triplets/s (triplets inside the
+cutoff evaluated per second, the count Simulation::GetNumParticleInteractions returns) and
+ms/step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c3|c3c15|c2|c1|c4] [--precision mixed|fp64]
+
+One process per GPU (torchrun for N > 1).  The path does not shard (one GPU holds the whole cell
+grid), so N GPUs run N independent replicas ("scaling": "weak"); no collective is on the data
+path, the only NCCL calls are the barrier and the max-over-ranks of the timed region.
+
+Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events on the stream the
+library runs on (torch's current stream, handed to the context), with a 256 MiB write between
+steps to flush L2 (the working set is smaller than L2).  `value` = all ranks' triplets / max over
+ranks of the summed step times.  `e2e` repeats the step through the C ABI with the particle state
+copied in from pinned host memory and back out every step.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    "c3": dict(desc="P3BCA, N=131072 uniform at density 2.048 (box 40^3), cutoff 2, 1 step/iteration",
+               algorithm="p3bca", n=131072, cutoff=2.0, gen="uniform"),
+    "c3c15": dict(desc="P3BCA, N=131072 uniform at density 2.048 (box 40^3), cutoff 1.5",
+                  algorithm="p3bca", n=131072, cutoff=1.5, gen="uniform"),
+    "c2": dict(desc="AUTA, N=8192 uniform in 20^3, no cutoff", algorithm="auta", n=8192, cutoff=0.0, gen="uniform",
+               box=20.0),
+    "c1": dict(desc="AUTA, N=512 uniform in 10^3, no cutoff", algorithm="auta", n=512, cutoff=0.0, gen="uniform",
+               box=10.0),
+    "c4": dict(desc="P3BCA, N=262144 clustered Gaussian (256 clusters, sigma 1) in 64^3, cutoff 2",
+               algorithm="p3bca", n=262144, cutoff=2.0, gen="clustered", box=64.0),
+}
+FLOP_PER_TRIPLET = 120  # the fixed, formulation-independent per-triplet credit (BASELINE convention)
+DT, G = 0.001, (0.0, -9.81, 0.0)
+
+
+def make_input(w):
+    from threebodymdalgorithms_b200 import generators as gen
+    if w["gen"] == "uniform":
+        side = w.get("box") or gen.box_for_density(w["n"], 2.048)
+        return gen.as_csv_values(gen.uniform(w["n"], (side, side, side), 1.0))
+    return gen.as_csv_values(gen.clustered_gauss(w["n"], 256, (w["box"],) * 3, 0.0, 1.0, 1.0))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def allreduce_max(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world):
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def timed_steps(ctx, steps, flush, torch):
+    """Per-step CUDA-event times (ms) on the context's stream, L2 flushed between steps."""
+    stream = torch.cuda.current_stream()
+    times, counts = [], []
+    for _ in range(steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        c = ctx.step(1)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        counts.append(int(c[0]))
+    return times, counts
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from threebodymdalgorithms_b200 import Context
+    from threebodymdalgorithms_b200._lib import load
+
+    w = WORKLOADS[args.workload]
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    st = make_input(w)
+    n = len(st["x"])
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def new_ctx(prec, graph=True):
+        c = Context(w["algorithm"], prec, w["cutoff"], DT, G, 1.0, device=local, use_graph=graph,
+                    stream=C.c_void_p(stream.cuda_stream))
+        c.set_state(st)
+        return c
+
+    result = {}
+    for prec in ([args.precision] + (["fp64"] if args.precision != "fp64" else [])):
+        ctx = new_ctx(prec)
+        if args.autotune:
+            ctx.autotune(str(ROOT / "profiles" / "autotune_cache.jsonl"))
+        timed_steps(ctx, args.warmup, flush, torch)
+        barrier(world)
+        l0 = ctx.kernel_launches()
+        with ClockSampler(local) as clk:
+            times, counts = timed_steps(ctx, args.steps, flush, torch)
+        launches = ctx.kernel_launches() - l0
+        barrier(world)
+        total_ms = allreduce_max(sum(times), world)
+        result[prec] = dict(times=times, counts=counts, total_ms=total_ms, launches=launches, clocks=clk.summary(),
+                            tuning=ctx.tuning())
+        # per-phase device times of the same steps (eager mode, events between phases)
+        ctx.set_profiling(True)
+        timed_steps(ctx, min(args.steps, 10), flush, torch)
+        result[prec]["phases"] = ctx.phase_times()
+        ctx.close()
+
+    main = result[args.precision]
+    trip_rank = float(sum(main["counts"]))
+    trip_all = allreduce_sum(trip_rank, world)
+    value = trip_all / (main["total_ms"] * 1e-3)
+    ms_per_step = main["total_ms"] / args.steps
+
+    # roofline of the dominant kernel (triplet forces), measured from the profiled pass
+    ph = main["phases"]["triplets"]
+    kern_ms = ph["ms"] / max(ph["calls"], 1)
+    mean_trip = trip_rank / args.steps
+    lib = load()
+    lib.tbmd_probe_fma_tflops.restype = C.c_double
+    lib.tbmd_probe_fma_tflops.argtypes = [C.c_int32, C.c_int32]
+    fp32_peak = lib.tbmd_probe_fma_tflops(local, 0)
+    fp64_peak = lib.tbmd_probe_fma_tflops(local, 1)
+    peak = fp32_peak if args.precision == "mixed" else fp64_peak
+    achieved = mean_trip * FLOP_PER_TRIPLET / (kern_ms * 1e-3) / 1e12
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        try:
+            traffic = json.loads(tfile.read_text()).get(f"{args.workload}:{args.precision}")
+        except (ValueError, OSError):
+            traffic = None
+    roofline = {"bound": "fp32" if args.precision == "mixed" else "fp64", "achieved": round(achieved, 3),
+                "peak": round(peak, 3), "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if peak > 0 else None,
+                "traffic": traffic, "kernel": "k_p3bca" if w["algorithm"] == "p3bca" else f"k_{w['algorithm']}",
+                "kernel_ms": round(kern_ms, 5), "flop_per_triplet": FLOP_PER_TRIPLET,
+                "peak_source": "measured on this GPU by tbmd_probe_fma_tflops (FMA = 2 FLOP)",
+                "phases_ms_per_step": {k: round(v["ms"] / max(v["calls"], 1), 5) for k, v in main["phases"].items()}}
+
+    # end to end through the C ABI with host buffers (pinned), per step: state in, step, state out
+    e2e = None
+    if not args.no_e2e:
+        ctx = new_ctx(args.precision)
+        pinned = {k: torch.from_numpy(np.ascontiguousarray(st[k], dtype=np.float64)).pin_memory().numpy()
+                  for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m")}
+        ids = torch.from_numpy(np.asarray(st["id"], dtype=np.int32)).pin_memory().numpy()
+        outs = {k: torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+                for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m", "fx", "fy", "fz")}
+        out_ids = torch.empty(n, dtype=torch.int32).pin_memory().numpy()
+        from threebodymdalgorithms_b200._lib import dptr
+        lib = ctx._lib
+
+        def e2e_step():
+            ctx._check(lib.tbmd_set_particles(ctx.handle, n, ids.ctypes.data_as(C.POINTER(C.c_int32)),
+                                              *[dptr(pinned[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "ax",
+                                                                          "ay", "az", "m")]))
+            c = ctx.step(1)
+            ctx._check(lib.tbmd_get_particles(ctx.handle, out_ids.ctypes.data_as(C.POINTER(C.c_int32)),
+                                              *[dptr(outs[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay",
+                                                                        "az", "m", "fx", "fy", "fz")]))
+            return int(c[0])
+
+        for _ in range(args.warmup):
+            e2e_step()
+        barrier(world)
+        e2e_ms, e2e_trip = [], 0
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            e2e_trip += e2e_step()
+            e1.record(stream)
+            e1.synchronize()
+            e2e_ms.append(e0.elapsed_time(e1))
+        barrier(world)
+        tot = allreduce_max(sum(e2e_ms), world)
+        e2e_all = allreduce_sum(float(e2e_trip), world)
+        e2e = {"value": e2e_all / (tot * 1e-3), "unit": "triplets/s", "ms_per_step": tot / args.steps,
+               "h2d_bytes_per_step": 10 * 8 * n + 4 * n, "d2h_bytes_per_step": 13 * 8 * n + 4 * n,
+               "path": "tbmd_set_particles + tbmd_step(1) + tbmd_get_particles, pinned host buffers"}
+        ctx.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w, st)
+
+    if rank == 0:
+        fp64 = result.get("fp64")
+        line = {
+            "metric": "triplets/s", "value": value, "unit": "triplets/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 geometry + f64 accumulation" if args.precision == "mixed" else "f64",
+            "data": "synthetic: the reference's particlegenerator sequences (mt19937 seed 926762934), 6-digit CSV values",
+            "config": {"workload": f"{args.workload}: {w['desc']}", "algorithm": w["algorithm"], "n": n,
+                       "cutoff": w["cutoff"], "precision": args.precision, "dt": DT, "g": list(G),
+                       "triplets_per_step": mean_trip, "l2": "flushed (256 MiB write) between timed steps",
+                       "parallelism": f"replicas x{world}", "graph": True, "tuning": main["tuning"]},
+            "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": main["launches"],
+            "clocks": main["clocks"],
+        }
+        if fp64 and args.precision != "fp64":
+            f_ms = fp64["total_ms"] / args.steps
+            line["fp64"] = {"ms_per_step": f_ms, "value": trip_all / (fp64["total_ms"] * 1e-3),
+                            "triplets_per_step": float(np.mean(fp64["counts"])),
+                            "phases_ms_per_step": {k: round(v["ms"] / max(v["calls"], 1), 5)
+                                                   for k, v in fp64["phases"].items()},
+                            "fp64_peak_tflops": round(fp64_peak, 3)}
+            line["speedup_mixed_vs_fp64"] = f_ms / ms_per_step
+            line["counts_equal_fp64_vs_mixed"] = fp64["counts"] == main["counts"]
+        print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(w, st):
+    """The oracle (OpenMP restatement of the reference loop with a cell list) on this host's cores,
+    one full step of the workload (bounded: about 1-20 s)."""
+    from oracle import oracle as O
+    O.build()
+    cores = os.cpu_count() or 1
+    if w["algorithm"] == "p3bca":
+        sample = dict(st)
+        label = f"one full step of the workload (N={len(st['x'])})"
+    else:
+        k = min(len(st["x"]), 1024)
+        sample = {key: v[:k] for key, v in st.items()}
+        label = f"first {k} particles of the workload, one step"
+    t = time.perf_counter()
+    _, counts = O.simulate(w["algorithm"], 1, sample, DT, G, w["cutoff"], 1.0, nthreads=cores)
+    dt = time.perf_counter() - t
+    return {"value": float(counts[0]) / dt, "unit": "triplets/s", "cores": cores, "kind": "port", "sample": label,
+            "seconds": dt}
+
+
+def run_reference(args, world, rank):
+    """The reference's own CPU code (built from its sources into oracle/_ref) on a bounded sample
+    of the workload: a cube of the workload's particles at the same density and cutoff, sized so
+    one step takes a few seconds.  Its loop is O(N^3) in candidates, so the full-size step is
+    extrapolated by the candidate count C(N,3)/C(n,3) and both numbers are reported."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    w = WORKLOADS[args.workload]
+    if not O.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference built from its sources) "
+                          "is missing on this machine"}), flush=True)
+        return
+    st = make_input(w)
+    N = len(st["x"])
+    budget = min(10.0, 150.0 / max(args.steps + args.warmup, 1))
+
+    def sample(k):
+        if w["algorithm"] == "p3bca":
+            d = (st["x"] - st["x"].min()) ** 2 + (st["y"] - st["y"].min()) ** 2 + (st["z"] - st["z"].min()) ** 2
+            idx = np.sort(np.argsort(d, kind="stable")[:k])  # a corner chunk at the workload's density
+        else:
+            idx = np.arange(min(k, N))
+        return {key: v[idx] for key, v in st.items()}
+
+    def run(s):
+        from threebodymdalgorithms_b200 import csvio
+        with tempfile.TemporaryDirectory() as tmp:
+            path = str(Path(tmp) / "in.csv")
+            csvio.write_input(path, s)
+            _, counts, secs = O.reference_dump(path, w["algorithm"], "sim", 1, DT, G, w["cutoff"], 1.0)
+        return int(counts[0]), secs
+
+    k = 256
+    _, secs = run(sample(k))
+    rate = math.comb(k, 3) / max(secs, 1e-6)  # candidate triplets per second
+    while k < N and math.comb(2 * k, 3) / rate < budget:
+        k *= 2
+    k = min(k, N)
+    s = sample(k)
+    for _ in range(args.warmup):
+        run(s)
+    trips, total = 0, 0.0
+    for _ in range(args.steps):
+        c, secs = run(s)
+        trips += c
+        total += secs
+    sample_rate = trips / total
+    per_step_sample = total / args.steps
+    full_trip = WORKLOAD_TRIPLETS.get(args.workload)
+    ext_step = per_step_sample * math.comb(N, 3) / math.comb(k, 3)
+    value = (full_trip / ext_step) if full_trip else sample_rate
+    line = {"impl": "reference", "metric": "triplets/s", "value": value, "unit": "triplets/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ext_step * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {w['desc']}", "algorithm": w["algorithm"], "n": N,
+                       "cutoff": w["cutoff"]},
+            "cpu_baseline": {"value": value, "unit": "triplets/s", "cores": 1, "kind": "reference",
+                             "sample": f"{k} particles of the workload (same density/cutoff), reference O(N^3) loop, "
+                                       f"{sample_rate:.4g} triplets/s on the sample, {per_step_sample:.3g} s/step; "
+                                       f"full step extrapolated by C(N,3)/C(n,3). One rank: no MPI on this host."},
+            "sample_value": sample_rate,
+            "e2e": {"value": value, "unit": "triplets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# exact triplets per step of the full workloads (from the oracle; C1/C2 are C(N,3))
+WORKLOAD_TRIPLETS = {"c1": math.comb(512, 3), "c2": math.comb(8192, 3), "c3": 48272380}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="c3")
+    ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
+    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, world, rank)
+        return
+    world, rank, local = dist_setup()
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

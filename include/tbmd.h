@@ -1,0 +1,171 @@
+/*
+ * tbmd.h - C ABI of the B200 implementation of the Axilrod-Teller three-body hot path
+ * (NATA / AUTA / P3BCA force evaluation and the Simulation step that integrates it).
+ *
+ * Plain C: pointers and sizes only, no exceptions, no C++ or torch types.  All host arrays are
+ * owned by the caller and copied in or out during the call; the context owns all device memory
+ * (particle state, cell grid, neighbour lists, CUDA graph).  One context per host thread; every
+ * device operation of a context runs on that context's CUDA stream.
+ *
+ * Reference seams replaced (paths inside dmartin13/ThreeBodyMDAlgorithms):
+ *   Simulation ctor / Init / Start     src/simulation/Simulation.cpp:3-19, 28-81
+ *   Algorithm::SimulationStep          src/algorithm/Algorithm.hpp:60 (NATA.cpp:82-200,
+ *                                      AUTA.cpp:236-384, P3BCA.cpp:516-805)
+ *   Potential::CalculateForces         src/potential/Potential.hpp:25, AxilrodTeller.cpp:7-149
+ *   DomainDecomposition::Get/SetMyParticles, Update, UpdatePredictorStage, ResetForces
+ *                                      src/decomposition/DomainDecomposition.hpp:23-30
+ *   Simulation::GetNumParticleInteractions / GetNumBufferInteractions   Simulation.cpp:89-96
+ */
+#ifndef TBMD_H
+#define TBMD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TBMD_ABI_VERSION 1
+
+typedef struct tbmd_ctx tbmd_ctx;
+
+/* Status codes.  The reference prints a message and calls exit(1) on bad input
+ * (cli.hpp:57-59, P3BCA.cpp:54-69, AUTA.cpp:129); here every entry point returns a status and
+ * tbmd_last_error() holds the message. */
+typedef enum {
+    TBMD_OK = 0,
+    TBMD_INVALID_ARG = 1,     /* null pointer, bad enum, n out of range, dt/nu not finite */
+    TBMD_BAD_INPUT = 2,       /* NaN/inf coordinates or mass <= 0 */
+    TBMD_NOT_READY = 3,       /* no particles set */
+    TBMD_CAPACITY_RETRY = 4,  /* neighbour capacity still too small after the automatic retries */
+    TBMD_CUDA_ERROR = 5,      /* a CUDA runtime call failed; see tbmd_last_error */
+    TBMD_TIMEOUT = 6,         /* a bounded device-side wait gave up (the kernel returned early) */
+    TBMD_NO_DEVICE = 7        /* no CUDA device, or not an sm_100 device */
+} tbmd_status;
+
+/* Same numbering as the reference's AlgorithmType (src/utility/enums.hpp). */
+typedef enum { TBMD_NATA = 0, TBMD_P3BCA = 1, TBMD_AUTA = 2 } tbmd_algorithm;
+
+typedef enum {
+    TBMD_FP64 = 0,  /* drop-in: all arithmetic in FP64 */
+    TBMD_MIXED = 1  /* FP32 triplet geometry, FP64 displacements/accumulation/integration */
+} tbmd_precision;
+
+/* Simulation parameters: the reference's CLI values (cli.hpp:12-25) plus the GPU options. */
+typedef struct {
+    int32_t algorithm;  /* tbmd_algorithm */
+    int32_t precision;  /* tbmd_precision */
+    double cutoff;      /* P3BCA only; <= 0 means no cutoff, like the reference (Algorithm.cpp:94) */
+    double dt;          /* -d */
+    double g[3];        /* -gx -gy -gz */
+    double nu;          /* AT strength; the reference uses AxilrodTeller(1.0) (main.cpp:41,66,91) */
+    int32_t device;     /* CUDA device ordinal */
+    int32_t use_graph;  /* 1: capture multi-step runs in a CUDA graph */
+    void *stream;       /* cudaStream_t to run on, or NULL for a stream owned by the context */
+    int32_t reserved[8];
+} tbmd_config;
+
+/* Fill *cfg with the reference's defaults: AUTA, FP64, cutoff 0, dt 0, g 0, nu 1, device 0,
+ * graphs on, own stream. */
+void tbmd_config_init(tbmd_config *cfg);
+
+/* Simulation constructor + Init (Simulation.cpp:3-19). */
+tbmd_status tbmd_create(const tbmd_config *cfg, tbmd_ctx **out);
+void tbmd_destroy(tbmd_ctx *ctx);
+const char *tbmd_last_error(const tbmd_ctx *ctx);
+const char *tbmd_status_string(tbmd_status s);
+int32_t tbmd_abi_version(void);
+
+/* Load the particle set (the reference's CSV input, utility.cpp:14-24, as SoA host arrays).
+ * id may be NULL (0..n-1).  For P3BCA this also fixes the periodic domain from these positions:
+ * L = |(max + 1e-4) - (min - 1e-4)| per axis (RegularGridDecomposition.cpp:24-28, 135-166).
+ * Forces are reset to zero.  n must be >= 1. */
+tbmd_status tbmd_set_particles(tbmd_ctx *ctx, int64_t n, const int32_t *id, const double *x, const double *y,
+                               const double *z, const double *vx, const double *vy, const double *vz,
+                               const double *ax, const double *ay, const double *az, const double *m);
+
+/* Copy the current state out (DomainDecomposition::GetMyParticles, in input order).  Any pointer
+ * may be NULL to skip that field.  fx/fy/fz are the stored forces (+grad E, like the reference). */
+tbmd_status tbmd_get_particles(tbmd_ctx *ctx, int32_t *id, double *x, double *y, double *z, double *vx,
+                               double *vy, double *vz, double *ax, double *ay, double *az, double *m,
+                               double *fx, double *fy, double *fz);
+
+int64_t tbmd_num_particles(const tbmd_ctx *ctx);
+
+/* Simulation::Start for `iterations` steps (Simulation.cpp:28-81): per step predictor
+ * (structs.hpp:40-55), force reset + triplet forces (Algorithm::SimulationStep), update
+ * (structs.hpp:57-99).  triplets_per_step (may be NULL) receives, per step, the value the
+ * reference returns from GetNumParticleInteractions(step). */
+tbmd_status tbmd_step(tbmd_ctx *ctx, int32_t iterations, uint64_t *triplets_per_step);
+
+/* Algorithm::SimulationStep alone at the current positions, without integration (how the
+ * reference's tests call it, tests.cpp:539).  Writes the stored forces into the context and,
+ * if non-NULL, to fx/fy/fz, the total AT energy to *energy, the triplet count to *triplets. */
+tbmd_status tbmd_forces(tbmd_ctx *ctx, double *fx, double *fy, double *fz, double *energy, uint64_t *triplets);
+
+/* Adjoint of tbmd_forces (no reference counterpart).  Given cotangents gf on the stored forces and
+ * g_energy on the energy, returns gx = H gf + g_energy * f (H = Hessian of the AT energy; the
+ * triplet set is held fixed) and g_nu = (gf . f + g_energy * E) / nu.  Geometry is recomputed,
+ * nothing per triplet is stored.  Any output may be NULL. */
+tbmd_status tbmd_adjoint(tbmd_ctx *ctx, const double *gfx, const double *gfy, const double *gfz, double g_energy,
+                         double *gx, double *gy, double *gz, double *g_nu);
+
+/* Device-pointer variants for callers that already hold device memory (torch tensors).  They run
+ * asynchronously on `stream` (cudaStream_t; NULL = the context stream) with positions of length n
+ * given by the caller; the context's P3BCA domain is used (set it first with tbmd_set_domain or
+ * tbmd_set_particles).  energy and triplets are device scalars (may be NULL). */
+tbmd_status tbmd_forces_device(tbmd_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
+                               double *fx, double *fy, double *fz, double *energy, uint64_t *triplets, void *stream);
+tbmd_status tbmd_adjoint_device(tbmd_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
+                                const double *gfx, const double *gfy, const double *gfz, const double *g_energy,
+                                double *fx, double *fy, double *fz, double *energy, double *gx, double *gy,
+                                double *gz, void *stream);
+
+/* Fix the P3BCA periodic domain explicitly (L = box lengths, lo = lower corner). */
+tbmd_status tbmd_set_domain(tbmd_ctx *ctx, const double *L, const double *lo);
+/* Read the domain and the cell grid: dims = cells per axis (an axis shorter than 3 cutoffs is one
+ * cell), cell_of_particle[n] (may be NULL) = linear cell index (cz*dy + cy)*dx + cx of each
+ * particle at the current positions, in input order. */
+tbmd_status tbmd_cells(tbmd_ctx *ctx, int32_t *cell_of_particle, int32_t *dims, double *L, double *lo);
+
+/* Batched forces/energy (no reference counterpart): nsys independent systems packed back to back
+ * (system s owns particles offsets[s] .. offsets[s+1]-1), each with its own P3BCA domain
+ * (box[3*s .. 3*s+2] lengths, lo[3*s ..] lower corners; ignored without a cutoff), evaluated in
+ * one persistent launch.  Host arrays.  energy and triplets are per system (may be NULL). */
+tbmd_status tbmd_batch_forces(tbmd_ctx *ctx, int32_t nsys, const int64_t *offsets, const double *box,
+                              const double *lo, const double *x, const double *y, const double *z, double *fx,
+                              double *fy, double *fz, double *energy, uint64_t *triplets);
+/* Batched adjoint: per-system g_energy[s]; returns gx (H gf + g_energy f) and g_nu per system. */
+tbmd_status tbmd_batch_adjoint(tbmd_ctx *ctx, int32_t nsys, const int64_t *offsets, const double *box,
+                               const double *lo, const double *x, const double *y, const double *z,
+                               const double *gfx, const double *gfy, const double *gfz, const double *g_energy,
+                               double *gx, double *gy, double *gz, double *g_nu);
+
+/* Autotuner: times the kernel variants of this context's algorithm/precision at its current n and
+ * keeps the fastest.  Results are cached as JSON in cache_path (NULL: no file) keyed by GPU name,
+ * algorithm, precision and n bucket; a cached entry is reused without timing. */
+tbmd_status tbmd_autotune(tbmd_ctx *ctx, const char *cache_path);
+/* The variant in use, as a short JSON object (valid until the next call on ctx). */
+const char *tbmd_tuning(const tbmd_ctx *ctx);
+
+/* Per-phase device timing, the counterpart of the reference's PROFILE_3BMDA phase timers
+ * (Algorithm.hpp:33-38, main.cpp:127-451).  While on, steps run eagerly (no CUDA graph) with CUDA
+ * events between phases on the context stream; times accumulate until tbmd_set_profiling is
+ * called again.  Phases, in this order: 0 predictor, 1 cell build (counting sort), 2 neighbour
+ * lists, 3 triplet forces (the P3BCA kernel or the NATA/AUTA sweep), 4 update (incl. unsort and
+ * count bookkeeping).  tbmd_phase_times fills up to max entries of ms (milliseconds), calls (phase
+ * executions) and launches (kernels launched in the phase) and returns the number of phases. */
+tbmd_status tbmd_set_profiling(tbmd_ctx *ctx, int32_t on);
+int32_t tbmd_phase_times(const tbmd_ctx *ctx, double *ms, uint64_t *calls, uint64_t *launches, int32_t max);
+
+/* Wait for all work of the context's stream. */
+tbmd_status tbmd_sync(tbmd_ctx *ctx);
+
+/* Number of kernels this context has launched since creation (all of them are this library's). */
+uint64_t tbmd_kernel_launches(const tbmd_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TBMD_H */

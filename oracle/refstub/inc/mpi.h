@@ -64,12 +64,15 @@ typedef struct {
 #define TBMD_STUB_FIRST_DERIVED 16
 #define TBMD_STUB_MAX_TYPES 64
 
-static inline MPI_Aint *tbmd_stub_extents(void)
+/* One registry for the whole program: C++ inline functions share their static locals across
+ * translation units (the reference registers its Particle type in main.cpp and uses it in
+ * Simulation.cpp). */
+inline MPI_Aint *tbmd_stub_extents(void)
 {
     static MPI_Aint ext[TBMD_STUB_MAX_TYPES] = {0, 1, 4, 8, 1, 8, 8, 8, 4};
     return ext;
 }
-static inline int *tbmd_stub_next_type(void)
+inline int *tbmd_stub_next_type(void)
 {
     static int next = TBMD_STUB_FIRST_DERIVED;
     return &next;

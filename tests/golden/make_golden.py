@@ -14,6 +14,7 @@ Run in a container that has the reference sources:  python tests/golden/make_gol
 from __future__ import annotations
 
 import json
+import subprocess
 import sys
 import tempfile
 from pathlib import Path
@@ -104,6 +105,17 @@ def main():
             np.savez_compressed(OUT / f"{c['name']}.npz", counts=counts, meta=np.array(json.dumps(meta)), **arrays)
             if c["keep_csv"]:
                 Path(OUT / f"{c['name']}.csv").write_text(Path(csv).read_text())
+                # the reference's own executable on the same input: its per-step CSV output files
+                base = str(Path(tmp) / f"{c['name']}_cli.csv")
+                cmd = [str(O.REF_DIR / "ref_main"), "-a", c["algo"], "-i", str(c["iters"]), "-d", repr(c["dt"]),
+                       "-gx", repr(c["g"][0]), "-gy", repr(c["g"][1]), "-gz", repr(c["g"][2]), "-csv", csv,
+                       "-o", base]
+                if c["algo"] == "p3bca":
+                    cmd += ["-c", repr(c["cutoff"])]
+                subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
+                last = c["iters"] - 1
+                Path(OUT / f"{c['name']}_cli_out_{last}.csv").write_text(
+                    Path(tmp, f"{c['name']}_cli_{last}.csv").read_text())
             print(f"{c['name']:36s} n={len(inp['x']):5d} counts={counts.tolist()} ({secs:.2f}s)")
 
 

@@ -1,0 +1,47 @@
+"""The drop-in executable against the reference executable's own CSV output (golden files)."""
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from threebodymdalgorithms_b200 import csvio
+
+pytestmark = pytest.mark.gpu
+ROOT = Path(__file__).resolve().parents[1]
+MAIN = ROOT / "threebodymdalgorithms_b200" / "tbmd_main"
+GOLDEN = ROOT / "tests" / "golden"
+
+
+def run_main(args, cwd):
+    r = subprocess.run([str(MAIN), *args], capture_output=True, text=True, cwd=cwd)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return r
+
+
+@pytest.mark.parametrize("name,args,last", [
+    ("c1_auta_n512", ["-a", "auta", "-i", "1"], 0),
+    ("p3bca_n512_c2_3steps", ["-a", "p3bca", "-i", "3", "-c", "2.0"], 2),
+])
+def test_cli_output_matches_reference(name, args, last, tmp_path):
+    run_main(args + ["-d", "0.001", "-gx", "0", "-gy", "-9.81", "-gz", "0", "-csv", str(GOLDEN / f"{name}.csv"),
+                     "-o", str(tmp_path / "out.csv")], tmp_path)
+    mine = (tmp_path / f"out_{last}.csv").read_text().splitlines()
+    ref = (GOLDEN / f"{name}_cli_out_{last}.csv").read_text().splitlines()
+    assert mine[0] == ref[0] and len(mine) == len(ref)
+    # 6-digit text: identical except where an FP64 rounding difference crosses a print boundary
+    differing = [i for i in range(len(ref)) if mine[i] != ref[i]]
+    assert len(differing) <= 2, differing[:5]
+    a = csvio.read_particles(str(tmp_path / f"out_{last}.csv"))
+    b = csvio.read_particles(str(GOLDEN / f"{name}_cli_out_{last}.csv"))
+    for k in ("x", "vx", "ax"):
+        assert np.allclose(a[k], b[k], rtol=2e-6, atol=1e-12)
+
+
+def test_cli_mixed_and_dump(tmp_path):
+    run_main(["-a", "P3BCA", "-i", "2", "-c", "2", "-d", "0.001", "-gy", "-9.81", "-prec", "mixed",
+              "-csv", str(GOLDEN / "p3bca_n512_c2_3steps.csv"), "-dumpfull", str(tmp_path / "d.txt"),
+              "-op", str(tmp_path / "prof.json")], tmp_path)
+    lines = (tmp_path / "d.txt").read_text().splitlines()
+    assert lines[0].startswith("step 0 buffer 1 triplets 12982")
+    assert (tmp_path / "prof.json").read_text().startswith("[{\"allTimes\"")

@@ -1,0 +1,229 @@
+"""Parity of the CUDA path (through the C ABI) with the reference and its oracle.
+
+Bars: triplet counts and cell assignments bit-exact; FP64 forces/velocities/positions within
+rel-L2 1e-12 of the reference (different but exact-in-exact-arithmetic formulation and summation
+order); mixed precision within rel-L2 1e-5 on forces (the target tolerance) and 1e-6 on
+velocities/positions after the run.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import golden_io as GIO
+from threebodymdalgorithms_b200 import Context, generators
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+MIXED_FORCE_TOL = 1e-5
+MIXED_STATE_TOL = 1e-6
+STATE = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "fx", "fy", "fz")
+
+
+def rel_l2(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def gpu_run(inp, meta, precision, use_graph=True):
+    ctx = Context(meta["algo"], precision, meta["cutoff"], meta["dt"], meta["g"], meta["nu"], use_graph=use_graph)
+    ctx.set_state(inp)
+    if meta["mode"] == "forces":
+        fx, fy, fz, e, c = ctx.forces()
+        st = ctx.get_state()
+        counts = np.array([c], dtype=np.uint64)
+    else:
+        counts = ctx.step(meta["iters"])
+        st = ctx.get_state()
+    ctx.close()
+    return st, counts
+
+
+def check_state(st, out, force_tol, state_tol):
+    for k in STATE:
+        tol = force_tol if k.startswith("f") or k.startswith("a") else state_tol
+        err = rel_l2(st[k], out[k])
+        assert err <= tol, (k, err)
+
+
+@pytest.mark.parametrize("name", GIO.names())
+def test_golden_fp64(name):
+    inp, out, counts, meta = GIO.load(name)
+    st, c = gpu_run(inp, meta, "fp64")
+    assert np.array_equal(c, counts), (c, counts)
+    check_state(st, out, FP64_TOL, FP64_TOL)
+
+
+@pytest.mark.parametrize("name", GIO.names())
+def test_golden_mixed(name):
+    inp, out, counts, meta = GIO.load(name)
+    st, c = gpu_run(inp, meta, "mixed")
+    assert np.array_equal(c, counts), (c, counts)
+    check_state(st, out, MIXED_FORCE_TOL, MIXED_STATE_TOL)
+
+
+@pytest.mark.parametrize("name", ["p3bca_n512_c2_3steps", "nata_n256_3steps", "auta_n300_light_3steps"])
+def test_graph_and_eager_agree(name):
+    inp, out, counts, meta = GIO.load(name)
+    a, ca = gpu_run(inp, meta, "fp64", use_graph=True)
+    b, cb = gpu_run(inp, meta, "fp64", use_graph=False)
+    assert np.array_equal(ca, cb)
+    for k in STATE:
+        assert rel_l2(a[k], b[k]) <= 1e-13, k
+
+
+def test_nata_is_deterministic():
+    inp, out, counts, meta = GIO.load("nata_n256_3steps")
+    a, _ = gpu_run(inp, meta, "fp64")
+    b, _ = gpu_run(inp, meta, "fp64")
+    for k in STATE:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def forces_of(algo, precision, st, cutoff=0.0):
+    ctx = Context(algo, precision, cutoff)
+    ctx.set_state(st)
+    fx, fy, fz, e, c = ctx.forces()
+    ctx.close()
+    return np.stack([fx, fy, fz], 1), e, c
+
+
+def test_auta_vs_oracle_n1024():
+    st = generators.as_csv_values(generators.uniform(1024, (12, 12, 12)))
+    fx, fy, fz, c = O.forces(st["x"], st["y"], st["z"], 1.0, -1.0, nthreads=0)
+    ref = np.stack([fx, fy, fz], 1)
+    e_ref = O.energy(st["x"], st["y"], st["z"], 1.0, -1.0)
+    for algo in ("auta", "nata"):
+        f64, e64, c64 = forces_of(algo, "fp64", st)
+        fmx, emx, cmx = forces_of(algo, "mixed", st)
+        assert c64 == cmx == c == math.comb(1024, 3)
+        assert rel_l2(f64, ref) <= FP64_TOL
+        assert rel_l2(fmx, ref) <= MIXED_FORCE_TOL
+        assert abs(e64 - e_ref) <= 1e-12 * abs(e_ref)
+        assert abs(emx - e_ref) <= 1e-6 * abs(e_ref)
+
+
+def test_c2_n8192_nata_auta_fp64_mixed():
+    """C2 (N=8192 uniform in 20^3): the two GPU algorithms and both precisions agree; momentum
+    is conserved (sum of forces ~ 0) and the count is C(N,3)."""
+    st = generators.as_csv_values(generators.uniform(8192, (20, 20, 20)))
+    fa, ea, ca = forces_of("auta", "fp64", st)
+    fn, en, cn = forces_of("nata", "fp64", st)
+    fm, em, cm = forces_of("auta", "mixed", st)
+    fnm, enm, cnm = forces_of("nata", "mixed", st)
+    assert ca == cn == cm == cnm == math.comb(8192, 3) == 91592417280
+    assert rel_l2(fn, fa) <= FP64_TOL
+    assert rel_l2(fm, fa) <= MIXED_FORCE_TOL
+    assert rel_l2(fnm, fa) <= MIXED_FORCE_TOL
+    assert np.abs(fa.sum(0)).max() <= 1e-9 * np.abs(fa).max() * 8192
+    assert abs(ea - en) <= 1e-12 * abs(ea) and abs(em - ea) <= 1e-6 * abs(ea)
+
+
+@pytest.mark.parametrize("cutoff", [2.0, 1.5])
+def test_c3_p3bca_full_size_vs_oracle(cutoff):
+    """C3: N=131072 uniform at density 2.048 (box 40^3), counts bit-exact against the oracle's
+    cell list, forces within tolerance, cell assignment bit-exact."""
+    n = 131072
+    side = generators.box_for_density(n)
+    st = generators.as_csv_values(generators.uniform(n, (side, side, side)))
+    L, lo = O.domain(st["x"], st["y"], st["z"])
+    fx, fy, fz, c_ref = O.forces(st["x"], st["y"], st["z"], 1.0, cutoff, L, lo, nthreads=0)
+    ref = np.stack([fx, fy, fz], 1)
+    for prec, tol in (("fp64", FP64_TOL), ("mixed", MIXED_FORCE_TOL)):
+        ctx = Context("p3bca", prec, cutoff)
+        ctx.set_state(st)
+        gfx, gfy, gfz, e, c = ctx.forces()
+        assert c == c_ref, (prec, c, c_ref)
+        assert rel_l2(np.stack([gfx, gfy, gfz], 1), ref) <= tol, prec
+        cell, dims, gL, glo = ctx.cells()
+        ocell, odims = O.cell_assign(st["x"], st["y"], st["z"], cutoff, L, lo)
+        assert dims == odims and np.array_equal(gL, L) and np.array_equal(glo, lo)
+        assert np.array_equal(cell, ocell)
+        ctx.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_p3bca_ten_steps_vs_oracle(prec):
+    n = 16384
+    side = generators.box_for_density(n)
+    st = generators.as_csv_values(generators.uniform(n, (side, side, side)))
+    ref, counts = O.simulate("p3bca", 10, st, 0.001, (0.0, -9.81, 0.0), cutoff=2.0, nthreads=0)
+    ctx = Context("p3bca", prec, 2.0, 0.001, (0.0, -9.81, 0.0))
+    ctx.set_state(st)
+    c = ctx.step(10)
+    got = ctx.get_state()
+    ctx.close()
+    assert np.array_equal(c, counts)
+    check_state(got, ref, FP64_TOL if prec == "fp64" else MIXED_FORCE_TOL,
+                FP64_TOL if prec == "fp64" else MIXED_STATE_TOL)
+
+
+def test_energy_p3bca_vs_oracle():
+    n = 4096
+    side = generators.box_for_density(n)
+    st = generators.uniform(n, (side, side, side))
+    L, lo = O.domain(st["x"], st["y"], st["z"])
+    e_ref = O.energy(st["x"], st["y"], st["z"], 1.0, 2.0, L, lo)
+    _, e64, _ = forces_of("p3bca", "fp64", st, 2.0)
+    _, emx, _ = forces_of("p3bca", "mixed", st, 2.0)
+    assert abs(e64 - e_ref) <= 1e-12 * abs(e_ref)
+    assert abs(emx - e_ref) <= 1e-6 * abs(e_ref)
+
+
+def test_clustered_capacity_retry():
+    """Clustered input: the mean-density capacity estimate is far too small in the clusters, the
+    overflow is detected on the device and the evaluation is redone with a larger capacity."""
+    st = generators.clustered_gauss(8192, 16, (32, 32, 32))
+    L, lo = O.domain(st["x"], st["y"], st["z"])
+    fx, fy, fz, c_ref = O.forces(st["x"], st["y"], st["z"], 1.0, 2.0, L, lo, nthreads=0)
+    f, e, c = forces_of("p3bca", "fp64", st, 2.0)
+    assert c == c_ref
+    assert rel_l2(f, np.stack([fx, fy, fz], 1)) <= FP64_TOL
+    ctx = Context("p3bca", "mixed", 2.0, 0.001, (0, -9.81, 0))
+    ctx.set_state(st)
+    ref, counts = O.simulate("p3bca", 3, st, 0.001, (0.0, -9.81, 0.0), cutoff=2.0, nthreads=0)
+    assert np.array_equal(ctx.step(3), counts)
+    ctx.close()
+
+
+@pytest.mark.parametrize("n", [1, 2])
+def test_fewer_than_three_particles(n):
+    st = generators.uniform(n, (3, 3, 3))
+    for algo, cut in (("auta", 0.0), ("nata", 0.0), ("p3bca", 2.0)):
+        f, e, c = forces_of(algo, "fp64", st, cut)
+        assert c == 0 and not f.any() and e == 0.0
+
+
+def test_bad_inputs_are_rejected():
+    from threebodymdalgorithms_b200 import TbmdError
+    ctx = Context("auta")
+    st = generators.uniform(8, (3, 3, 3))
+    st["x"][3] = np.nan
+    with pytest.raises(TbmdError) as e:
+        ctx.set_state(st)
+    assert e.value.status == 2
+    st = generators.uniform(8, (3, 3, 3))
+    st["m"][0] = 0.0
+    with pytest.raises(TbmdError) as e:
+        ctx.set_state(st)
+    assert e.value.status == 2
+    with pytest.raises(TbmdError) as e:
+        ctx.step(1)
+    assert e.value.status == 3
+    ctx.close()
+
+
+def test_autotune_keeps_results(tmp_path):
+    st = generators.uniform(2048, (12, 12, 12))
+    ref, _, _ = forces_of("auta", "mixed", st)
+    ctx = Context("auta", "mixed")
+    ctx.set_state(st)
+    cache = tmp_path / "tune.jsonl"
+    t1 = ctx.autotune(str(cache))
+    t2 = ctx.autotune(str(cache))  # second call is served from the cache
+    assert t1 == t2 and cache.exists()
+    fx, fy, fz, e, c = ctx.forces()
+    assert rel_l2(np.stack([fx, fy, fz], 1), ref) <= MIXED_FORCE_TOL
+    ctx.close()

@@ -1,0 +1,1000 @@
+// C ABI (include/tbmd.h): context, particle state, the Simulation step loop, forces, adjoint,
+// device-pointer variants.  Host code in C++; every device operation is enqueued on the context
+// stream.  Multi-step runs are captured once per configuration as a CUDA graph of one step and
+// replayed; per-step triplet counts are recorded on the device and read back once per call.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/tbmd.h"
+#include "tbmd_internal.cuh"
+
+using namespace tbmd;
+
+namespace {
+
+constexpr double kCellMargin = 1.000001;  // cell width >= cutoff * margin (same constant as the oracle)
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t b)
+    {
+        if (b <= bytes && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, b ? b : 16);
+        if (e == cudaSuccess) bytes = b;
+        return e;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T *as() const { return (T *)p; }
+};
+
+}  // namespace
+
+struct tbmd_ctx {
+    tbmd_config cfg{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    std::string tuning;
+    uint64_t launches = 0;
+
+    int64_t n = 0;
+    std::vector<int32_t> id;
+
+    // particle state, 13 FP64 arrays of n: x y z vx vy vz ax ay az m fx fy fz
+    DevBuf state;
+    double *s[13] = {};
+    DevBuf snapshot;  // copy of x..az taken before a multi-step run (capacity retry)
+
+    // scalars: energy, count_cur, step counter, per-step counts
+    DevBuf scalars;
+    DevBuf step_counts;
+    int64_t step_counts_cap = 0;
+
+    // no-cutoff sweeps
+    int R_auta = 4, R_nata = 2, R_fp64 = 2;
+    DevBuf prefix;
+    int prefix_JB = 0, prefix_alg = -1;
+    int64_t prefix_n = -1;
+    int nblocks = 0;
+    int64_t total_items = 0;
+    DevBuf partial;
+    int sweep_grid = 0;
+
+    // P3BCA
+    bool domain_set = false;
+    double L[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
+    Grid grid{};
+    DevBuf cell_n, cell_c, nbr_buf;
+    int64_t cell_bufs_n = -1, cell_bufs_cells = -1;
+    CellBufs cb{};
+    int cap = 0;
+    int p3_warps = 4;
+    P3Plan plan{};
+
+    // adjoint / device-variant scratch
+    DevBuf dirs, hvp;
+
+    // phase profiling (eager mode): marks recorded on the stream, resolved after each sync
+    bool profiling = false;
+    std::vector<cudaEvent_t> event_pool;
+    std::vector<std::pair<int, cudaEvent_t>> marks;  // (phase that starts at this mark, event)
+    double phase_ms[5] = {0, 0, 0, 0, 0};
+    uint64_t phase_calls[5] = {0, 0, 0, 0, 0};
+    uint64_t phase_launches[5] = {0, 0, 0, 0, 0};
+    int cur_phase = -1;
+    int cur_phase_launch0 = 0;
+
+    // graph of one step
+    cudaGraphExec_t gexec = nullptr;
+    bool graph_valid = false;
+    int graph_launches_per_step = 0;
+};
+
+// ---------------------------------------------------------------------------------------------
+// helpers
+
+static tbmd_status fail(tbmd_ctx *c, tbmd_status s, const char *fmt, ...)
+{
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        c->err = buf;
+    }
+    return s;
+}
+
+#define CK(call)                                                                                             \
+    do {                                                                                                     \
+        cudaError_t e_ = (call);                                                                             \
+        if (e_ != cudaSuccess) return fail(ctx, TBMD_CUDA_ERROR, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                                           __FILE__, __LINE__);                                              \
+    } while (0)
+
+static bool is_p3bca_cut(const tbmd_ctx *ctx) { return ctx->cfg.algorithm == TBMD_P3BCA && ctx->cfg.cutoff > 0; }
+static bool mixed(const tbmd_ctx *ctx) { return ctx->cfg.precision == TBMD_MIXED; }
+
+static unsigned long long choose3(int64_t n)
+{
+    if (n < 3) return 0;
+    unsigned __int128 v = (unsigned __int128)n * (unsigned __int128)(n - 1) * (unsigned __int128)(n - 2) / 6;
+    return v > (unsigned __int128)UINT64_MAX ? UINT64_MAX : (unsigned long long)v;
+}
+
+static double *energy_ptr(tbmd_ctx *c) { return c->scalars.as<double>(); }
+static unsigned long long *count_ptr(tbmd_ctx *c) { return (unsigned long long *)(c->scalars.as<char>() + 8); }
+static unsigned int *step_ptr(tbmd_ctx *c) { return (unsigned int *)(c->scalars.as<char>() + 16); }
+static unsigned int *sweep_counter(tbmd_ctx *c) { return (unsigned int *)(c->scalars.as<char>() + 24); }
+
+static int sweep_R(const tbmd_ctx *ctx)
+{
+    if (!mixed(ctx)) return ctx->R_fp64;
+    return ctx->cfg.algorithm == TBMD_NATA ? ctx->R_nata : ctx->R_auta;
+}
+
+static void invalidate_graph(tbmd_ctx *ctx)
+{
+    if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+    ctx->gexec = nullptr;
+    ctx->graph_valid = false;
+}
+
+enum Phase { PH_PREDICTOR = 0, PH_CELLS = 1, PH_NEIGHBORS = 2, PH_TRIPLETS = 3, PH_UPDATE = 4, PH_END = -1 };
+
+// Start a profiling phase (or end the current one with PH_END).  nl = launches so far in this
+// enqueue; the difference is attributed to the phase that ends.
+static void phase_mark(tbmd_ctx *ctx, cudaStream_t st, int phase, int nl)
+{
+    if (!ctx->profiling) return;
+    if (ctx->cur_phase >= 0) ctx->phase_launches[ctx->cur_phase] += (uint64_t)(nl - ctx->cur_phase_launch0);
+    cudaEvent_t e;
+    if (ctx->event_pool.empty()) {
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+    } else {
+        e = ctx->event_pool.back();
+        ctx->event_pool.pop_back();
+    }
+    cudaEventRecord(e, st);
+    ctx->marks.push_back({phase, e});
+    ctx->cur_phase = phase;
+    ctx->cur_phase_launch0 = nl;
+    if (phase >= 0) ctx->phase_calls[phase] += 1;
+}
+
+// After a synchronisation: add the elapsed time between consecutive marks to their phases.
+static void phase_resolve(tbmd_ctx *ctx)
+{
+    for (size_t k = 0; k + 1 < ctx->marks.size(); ++k) {
+        int ph = ctx->marks[k].first;
+        float ms = 0.f;
+        if (ph >= 0 && cudaEventElapsedTime(&ms, ctx->marks[k].second, ctx->marks[k + 1].second) == cudaSuccess)
+            ctx->phase_ms[ph] += ms;
+    }
+    for (auto &m : ctx->marks) ctx->event_pool.push_back(m.second);
+    ctx->marks.clear();
+    ctx->cur_phase = -1;
+}
+
+// Work list of the no-cutoff sweep for (algorithm, n, R).
+static tbmd_status ensure_sweep(tbmd_ctx *ctx, int alg, int64_t n, int R, bool dual)
+{
+    const int JB = 32 * R;
+    if (ctx->prefix_n != n || ctx->prefix_JB != JB || ctx->prefix_alg != alg) {
+        std::vector<int64_t> pre((size_t)(n / JB + 3), 0);
+        int64_t total = sweep_items(alg, n, JB, pre.data());
+        int64_t nb = n >= 3 ? (n - 2 + JB) / JB : 0;
+        if (total >= (int64_t)UINT32_MAX - 65536)
+            return fail(ctx, TBMD_INVALID_ARG, "n = %lld gives too many sweep work items", (long long)n);
+        CK(ctx->prefix.ensure(sizeof(int64_t) * (nb + 1)));
+        CK(cudaMemcpyAsync(ctx->prefix.p, pre.data(), sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        ctx->prefix_n = n;
+        ctx->prefix_JB = JB;
+        ctx->prefix_alg = alg;
+        ctx->nblocks = (int)nb;
+        ctx->total_items = total;
+        if (alg == TBMD_NATA) CK(ctx->partial.ensure(sizeof(double) * 3 * (size_t)n * (size_t)(nb > 0 ? nb : 1)));
+    }
+    int per_sm = 0, sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    (void)dual;
+    per_sm = 2048 / sweep_block_size(alg, mixed(ctx), dual, R);  // resident blocks bounded below by registers
+    if (per_sm < 1) per_sm = 1;
+    ctx->sweep_grid = sms * per_sm;
+    return TBMD_OK;
+}
+
+// Cell grid for the current domain and cutoff (oracle tbo_cell_dims).
+static void make_grid(tbmd_ctx *ctx)
+{
+    Grid &g = ctx->grid;
+    for (int d = 0; d < 3; ++d) {
+        double m = std::floor(ctx->L[d] / (ctx->cfg.cutoff * kCellMargin));
+        int nd = (m >= 3.0) ? (m > 1024.0 ? 1024 : (int)m) : 1;
+        g.dims[d] = nd;
+        g.L[d] = ctx->L[d];
+        g.lo[d] = ctx->lo[d];
+        g.w[d] = ctx->L[d] / (double)nd;
+    }
+    g.ncells = (int64_t)g.dims[0] * g.dims[1] * g.dims[2];
+    g.sqcut = ctx->cfg.cutoff * ctx->cfg.cutoff;
+}
+
+// Neighbour-list capacity estimate from the mean density: twice the expected half-list length
+// plus slack, rounded to 32.  Clustered inputs are corrected by the overflow retry.
+static int initial_cap(const tbmd_ctx *ctx, int64_t n)
+{
+    double vol = ctx->L[0] * ctx->L[1] * ctx->L[2];
+    double rho = vol > 0 ? (double)n / vol : 0.0;
+    double c = ctx->cfg.cutoff;
+    double half = 4.18879020478639 * c * c * c * rho * 0.5;
+    double want = 2.0 * half + 48.0;
+    if (want > (double)n) want = (double)n + 32;
+    int cap = ((int)want + 31) / 32 * 32;
+    return cap < 32 ? 32 : cap;
+}
+
+static tbmd_status ensure_cells(tbmd_ctx *ctx, int64_t n, bool dual, bool energy)
+{
+    if (!ctx->domain_set)
+        return fail(ctx, TBMD_NOT_READY, "P3BCA needs a domain: set particles or call tbmd_set_domain");
+    make_grid(ctx);
+    const int64_t nc = ctx->grid.ncells;
+    if (ctx->cap == 0) ctx->cap = initial_cap(ctx, n);
+    if (ctx->cell_bufs_n != n || ctx->cell_bufs_cells != nc) {
+        // per particle: FP64 xs ys zs dxs dys dzs fs[3] hs[3]; int32 cell_of, sorted, nbr_count
+        CK(ctx->cell_n.ensure((size_t)n * (12 * sizeof(double) + 3 * sizeof(int32_t)) + 256));
+        CK(ctx->cell_c.ensure((size_t)(3 * nc + 1) * sizeof(int32_t) + 256));
+        double *d = ctx->cell_n.as<double>();
+        CellBufs &cb = ctx->cb;
+        cb.xs = d;
+        cb.ys = d + n;
+        cb.zs = d + 2 * n;
+        cb.dxs = d + 3 * n;
+        cb.dys = d + 4 * n;
+        cb.dzs = d + 5 * n;
+        for (int k = 0; k < 3; ++k) {
+            cb.fs[k] = d + (6 + k) * n;
+            cb.hs[k] = d + (9 + k) * n;
+        }
+        int32_t *q = (int32_t *)(d + 12 * n);
+        cb.cell_of = q;
+        cb.sorted = q + n;
+        cb.nbr_count = q + 2 * n;
+        int32_t *r = ctx->cell_c.as<int32_t>();
+        cb.cell_count = r;
+        cb.cell_fill = r + nc;
+        cb.cell_start = r + 2 * nc;
+        ctx->cell_bufs_n = n;
+        ctx->cell_bufs_cells = nc;
+    }
+    CK(ctx->nbr_buf.ensure((size_t)n * ctx->cap * sizeof(int32_t) + 64));
+    ctx->cb.nbr = ctx->nbr_buf.as<int32_t>();
+    ctx->cb.max_count = (int32_t *)(ctx->scalars.as<char>() + 28);
+    ctx->cb.work_counter = (unsigned int *)(ctx->scalars.as<char>() + 32);
+    ctx->cb.cap = ctx->cap;
+    CK(plan_p3bca(mixed(ctx), dual, energy, ctx->cap, ctx->p3_warps, &ctx->plan));
+    return TBMD_OK;
+}
+
+static tbmd_status ensure_scalars(tbmd_ctx *ctx)
+{
+    if (!ctx->scalars.p) {
+        CK(ctx->scalars.ensure(64));
+        CK(cudaMemsetAsync(ctx->scalars.p, 0, 64, ctx->stream));
+    }
+    return TBMD_OK;
+}
+
+// Prepare buffers for a forward (or adjoint) evaluation of n particles.
+static tbmd_status prepare(tbmd_ctx *ctx, int64_t n, bool dual, bool energy)
+{
+    tbmd_status s = ensure_scalars(ctx);
+    if (s != TBMD_OK) return s;
+    if (is_p3bca_cut(ctx)) return ensure_cells(ctx, n, dual, energy);
+    const int alg = dual ? TBMD_AUTA : (ctx->cfg.algorithm == TBMD_NATA ? TBMD_NATA : TBMD_AUTA);
+    const int R = dual ? (mixed(ctx) ? 2 : 1) : sweep_R(ctx);
+    return ensure_sweep(ctx, alg, n, R, dual);
+}
+
+__global__ void k_add_u64(unsigned long long *p, unsigned long long v) { *p += v; }
+
+// Enqueue the triplet forces of n particles at `pos` into `out` (f, and H*d when dual).  The
+// outputs are overwritten.  energy (may be NULL) and count accumulate on the device.
+static tbmd_status enqueue_forces(tbmd_ctx *ctx, int64_t n, Pos pos, Out out, bool dual, double *energy,
+                                  unsigned long long *count, cudaStream_t st, int *nl)
+{
+    const double nu = ctx->cfg.nu;
+    const bool mx = mixed(ctx);
+    if (n <= 0) return TBMD_OK;
+    if (is_p3bca_cut(ctx)) {
+        CellBufs &cb = ctx->cb;
+        phase_mark(ctx, st, PH_CELLS, *nl);
+        CK(launch_cell_build(n, pos, ctx->grid, cb, dual, st, nl));
+        phase_mark(ctx, st, PH_NEIGHBORS, *nl);
+        CK(launch_neighbors(n, ctx->grid, cb, st));
+        *nl += 1;
+        for (int k = 0; k < 3; ++k) {
+            CK(cudaMemsetAsync(cb.fs[k], 0, sizeof(double) * n, st));
+            if (dual) CK(cudaMemsetAsync(cb.hs[k], 0, sizeof(double) * n, st));
+        }
+        phase_mark(ctx, st, PH_TRIPLETS, *nl);
+        CK(launch_p3bca(mx, dual, energy != nullptr, n, ctx->grid, cb, nu, energy, count, ctx->plan, st));
+        *nl += 1;
+        phase_mark(ctx, st, PH_UPDATE, *nl);
+        CK(launch_unsort(n, cb, out, dual, st));
+        *nl += 1 + (dual ? 1 : 0);
+        return TBMD_OK;
+    }
+    phase_mark(ctx, st, PH_TRIPLETS, *nl);
+    SweepWork w{ctx->prefix.as<int64_t>(), ctx->nblocks, ctx->total_items, sweep_counter(ctx)};
+    CK(cudaMemsetAsync(w.counter, 0, sizeof(unsigned int), st));
+    if (ctx->cfg.algorithm == TBMD_NATA && !dual) {
+        CK(launch_nata(mx, false, ctx->prefix_JB / 32, energy != nullptr, n, pos, out, energy, nu, w,
+                       ctx->partial.as<double>(), ctx->sweep_grid, st));
+        *nl += 1;
+        phase_mark(ctx, st, PH_UPDATE, *nl);
+        CK(launch_nata_reduce(false, n, ctx->nblocks, ctx->partial.as<double>(), out, st));
+        *nl += 1;
+    } else {
+        CK(cudaMemsetAsync(out.fx, 0, sizeof(double) * n, st));
+        CK(cudaMemsetAsync(out.fy, 0, sizeof(double) * n, st));
+        CK(cudaMemsetAsync(out.fz, 0, sizeof(double) * n, st));
+        if (dual) {
+            CK(cudaMemsetAsync(out.hx, 0, sizeof(double) * n, st));
+            CK(cudaMemsetAsync(out.hy, 0, sizeof(double) * n, st));
+            CK(cudaMemsetAsync(out.hz, 0, sizeof(double) * n, st));
+        }
+        CK(launch_auta(mx, dual, ctx->prefix_JB / 32, energy != nullptr, n, pos, out, energy, nu, w, ctx->sweep_grid,
+                       st));
+        *nl += 1;
+        phase_mark(ctx, st, PH_UPDATE, *nl);
+    }
+    if (count) {
+        k_add_u64<<<1, 1, 0, st>>>(count, choose3(n));
+        CK(cudaGetLastError());
+        *nl += 1;
+    }
+    return TBMD_OK;
+}
+
+static Pos state_pos(tbmd_ctx *c) { return Pos{c->s[0], c->s[1], c->s[2], nullptr, nullptr, nullptr}; }
+static Out state_out(tbmd_ctx *c) { return Out{c->s[10], c->s[11], c->s[12], nullptr, nullptr, nullptr}; }
+
+// One Simulation::Start iteration: predictor, forces, update, per-step count.
+static tbmd_status enqueue_step(tbmd_ctx *ctx, cudaStream_t st, int *nl)
+{
+    const int64_t n = ctx->n;
+    double **s = ctx->s;
+    phase_mark(ctx, st, PH_PREDICTOR, *nl);
+    CK(launch_predictor(n, s[0], s[1], s[2], s[3], s[4], s[5], s[6], ctx->cfg.dt, st));
+    *nl += 1;
+    // forces of the step's count go to count_cur; the no-cutoff count C(n,3) is added by k_add_u64
+    tbmd_status r = enqueue_forces(ctx, n, state_pos(ctx), state_out(ctx), false, nullptr, count_ptr(ctx), st, nl);
+    if (r != TBMD_OK) return r;
+    CK(launch_update(n, s[3], s[4], s[5], s[6], s[7], s[8], s[10], s[11], s[12], s[9], ctx->cfg.dt, ctx->cfg.g[0],
+                     ctx->cfg.g[1], ctx->cfg.g[2], st));
+    CK(launch_record_count(count_ptr(ctx), ctx->step_counts.as<unsigned long long>(), step_ptr(ctx), 0ull, st));
+    *nl += 2;
+    phase_mark(ctx, st, PH_END, *nl);
+    return TBMD_OK;
+}
+
+static tbmd_status build_graph(tbmd_ctx *ctx)
+{
+    invalidate_graph(ctx);
+    cudaGraph_t g = nullptr;
+    int nl = 0;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    tbmd_status r = enqueue_step(ctx, ctx->stream, &nl);
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (r != TBMD_OK) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e != cudaSuccess) return fail(ctx, TBMD_CUDA_ERROR, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&ctx->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(ctx, TBMD_CUDA_ERROR, "graph instantiate: %s", cudaGetErrorString(e));
+    ctx->graph_valid = true;
+    ctx->graph_launches_per_step = nl;
+    return TBMD_OK;
+}
+
+static tbmd_status check_device(tbmd_ctx *ctx)
+{
+    CK(cudaSetDevice(ctx->device));
+    return TBMD_OK;
+}
+
+static bool finite3(const double *a, int64_t n)
+{
+    for (int64_t i = 0; i < n; ++i)
+        if (!std::isfinite(a[i])) return false;
+    return true;
+}
+
+// ---------------------------------------------------------------------------------------------
+// C ABI
+
+extern "C" {
+
+void tbmd_config_init(tbmd_config *cfg)
+{
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof *cfg);
+    cfg->algorithm = TBMD_AUTA;
+    cfg->precision = TBMD_FP64;
+    cfg->nu = 1.0;
+    cfg->use_graph = 1;
+}
+
+int32_t tbmd_abi_version(void) { return TBMD_ABI_VERSION; }
+
+const char *tbmd_status_string(tbmd_status s)
+{
+    switch (s) {
+        case TBMD_OK: return "ok";
+        case TBMD_INVALID_ARG: return "invalid argument";
+        case TBMD_BAD_INPUT: return "bad input";
+        case TBMD_NOT_READY: return "not ready";
+        case TBMD_CAPACITY_RETRY: return "neighbour capacity exceeded";
+        case TBMD_CUDA_ERROR: return "CUDA error";
+        case TBMD_TIMEOUT: return "device wait timed out";
+        case TBMD_NO_DEVICE: return "no sm_100 CUDA device";
+    }
+    return "unknown status";
+}
+
+const char *tbmd_last_error(const tbmd_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+tbmd_status tbmd_create(const tbmd_config *cfg, tbmd_ctx **out)
+{
+    if (!cfg || !out) return TBMD_INVALID_ARG;
+    *out = nullptr;
+    if (cfg->algorithm < 0 || cfg->algorithm > 2 || cfg->precision < 0 || cfg->precision > 1)
+        return TBMD_INVALID_ARG;
+    if (!std::isfinite(cfg->dt) || !std::isfinite(cfg->nu) || !std::isfinite(cfg->cutoff) ||
+        !std::isfinite(cfg->g[0]) || !std::isfinite(cfg->g[1]) || !std::isfinite(cfg->g[2]))
+        return TBMD_INVALID_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || cfg->device < 0 || cfg->device >= ndev) {
+        cudaGetLastError();
+        return TBMD_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess || prop.major != 10) return TBMD_NO_DEVICE;
+    tbmd_ctx *ctx = new (std::nothrow) tbmd_ctx();
+    if (!ctx) return TBMD_INVALID_ARG;
+    ctx->cfg = *cfg;
+    ctx->device = cfg->device;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        delete ctx;
+        return TBMD_NO_DEVICE;
+    }
+    if (cfg->stream) {
+        ctx->stream = (cudaStream_t)cfg->stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete ctx;
+            return TBMD_CUDA_ERROR;
+        }
+        ctx->own_stream = true;
+    }
+    if (ensure_scalars(ctx) != TBMD_OK) {
+        tbmd_destroy(ctx);
+        return TBMD_CUDA_ERROR;
+    }
+    ctx->tuning = "{}";
+    *out = ctx;
+    return TBMD_OK;
+}
+
+void tbmd_destroy(tbmd_ctx *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    invalidate_graph(ctx);
+    for (auto &m : ctx->marks) cudaEventDestroy(m.second);
+    for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+    for (DevBuf *b : {&ctx->state, &ctx->snapshot, &ctx->scalars, &ctx->step_counts, &ctx->prefix, &ctx->partial,
+                      &ctx->cell_n, &ctx->cell_c, &ctx->nbr_buf, &ctx->dirs, &ctx->hvp})
+        b->release();
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int64_t tbmd_num_particles(const tbmd_ctx *ctx) { return ctx ? ctx->n : 0; }
+uint64_t tbmd_kernel_launches(const tbmd_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+tbmd_status tbmd_set_particles(tbmd_ctx *ctx, int64_t n, const int32_t *id, const double *x, const double *y,
+                               const double *z, const double *vx, const double *vy, const double *vz,
+                               const double *ax, const double *ay, const double *az, const double *m)
+{
+    if (!ctx) return TBMD_INVALID_ARG;
+    if (n < 1 || n > (int64_t)INT32_MAX / 2) return fail(ctx, TBMD_INVALID_ARG, "n = %lld out of range", (long long)n);
+    const double *src[10] = {x, y, z, vx, vy, vz, ax, ay, az, m};
+    for (int k = 0; k < 10; ++k)
+        if (!src[k]) return fail(ctx, TBMD_INVALID_ARG, "null particle array %d", k);
+    for (int k = 0; k < 10; ++k)
+        if (!finite3(src[k], n)) return fail(ctx, TBMD_BAD_INPUT, "non-finite value in particle array %d", k);
+    for (int64_t i = 0; i < n; ++i)
+        if (!(m[i] > 0)) return fail(ctx, TBMD_BAD_INPUT, "mass of particle %lld is not positive", (long long)i);
+    tbmd_status st = check_device(ctx);
+    if (st != TBMD_OK) return st;
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->n != n) invalidate_graph(ctx);
+    CK(ctx->state.ensure(sizeof(double) * 13 * (size_t)n));
+    for (int k = 0; k < 13; ++k) ctx->s[k] = ctx->state.as<double>() + (size_t)k * n;
+    for (int k = 0; k < 10; ++k)
+        CK(cudaMemcpyAsync(ctx->s[k], src[k], sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(ctx->s[10], 0, sizeof(double) * 3 * n, ctx->stream));
+    ctx->id.resize(n);
+    for (int64_t i = 0; i < n; ++i) ctx->id[i] = id ? id[i] : (int32_t)i;
+    ctx->n = n;
+    if (ctx->cfg.algorithm == TBMD_P3BCA) {
+        // RegularGridDecomposition::getDomainMinMax + Init, from these (initial) positions
+        const double *p[3] = {x, y, z};
+        for (int d = 0; d < 3; ++d) {
+            double mn = p[d][0], mxv = p[d][0];
+            for (int64_t i = 1; i < n; ++i) {
+                if (p[d][i] < mn) mn = p[d][i];
+                if (p[d][i] > mxv) mxv = p[d][i];
+            }
+            double a = mn - 0.0001, b = mxv + 0.0001;
+            ctx->lo[d] = a;
+            ctx->L[d] = std::fabs(b - a);
+        }
+        ctx->domain_set = true;
+        ctx->cap = 0;
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TBMD_OK;
+}
+
+tbmd_status tbmd_set_domain(tbmd_ctx *ctx, const double *L, const double *lo)
+{
+    if (!ctx || !L || !lo) return TBMD_INVALID_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (!(L[d] > 0) || !std::isfinite(L[d]) || !std::isfinite(lo[d]))
+            return fail(ctx, TBMD_INVALID_ARG, "bad domain on axis %d", d);
+    for (int d = 0; d < 3; ++d) {
+        ctx->L[d] = L[d];
+        ctx->lo[d] = lo[d];
+    }
+    ctx->domain_set = true;
+    ctx->cap = 0;
+    invalidate_graph(ctx);
+    return TBMD_OK;
+}
+
+tbmd_status tbmd_get_particles(tbmd_ctx *ctx, int32_t *id, double *x, double *y, double *z, double *vx, double *vy,
+                               double *vz, double *ax, double *ay, double *az, double *m, double *fx, double *fy,
+                               double *fz)
+{
+    if (!ctx) return TBMD_INVALID_ARG;
+    if (ctx->n == 0) return fail(ctx, TBMD_NOT_READY, "no particles set");
+    tbmd_status st = check_device(ctx);
+    if (st != TBMD_OK) return st;
+    double *dst[13] = {x, y, z, vx, vy, vz, ax, ay, az, m, fx, fy, fz};
+    for (int k = 0; k < 13; ++k)
+        if (dst[k]) CK(cudaMemcpyAsync(dst[k], ctx->s[k], sizeof(double) * ctx->n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (id) std::memcpy(id, ctx->id.data(), sizeof(int32_t) * ctx->n);
+    return TBMD_OK;
+}
+
+// Grow the neighbour capacity after an overflow; true if a retry is worthwhile.
+static bool grow_cap(tbmd_ctx *ctx, int32_t seen)
+{
+    if (seen <= ctx->cap) return false;
+    int want = (int)((double)seen * 1.25) + 32;
+    ctx->cap = (want + 31) / 32 * 32;
+    invalidate_graph(ctx);
+    return true;
+}
+
+tbmd_status tbmd_step(tbmd_ctx *ctx, int32_t iterations, uint64_t *counts)
+{
+    if (!ctx) return TBMD_INVALID_ARG;
+    if (iterations < 0) return fail(ctx, TBMD_INVALID_ARG, "iterations < 0");
+    if (ctx->n == 0) return fail(ctx, TBMD_NOT_READY, "no particles set");
+    if (iterations == 0) return TBMD_OK;
+    tbmd_status st = check_device(ctx);
+    if (st != TBMD_OK) return st;
+    if (ctx->step_counts_cap < iterations) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        CK(ctx->step_counts.ensure(sizeof(unsigned long long) * iterations));
+        ctx->step_counts_cap = iterations;
+        invalidate_graph(ctx);
+    }
+    const bool cut = is_p3bca_cut(ctx);
+    const int64_t n = ctx->n;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        void *before[4] = {ctx->state.p, ctx->nbr_buf.p, ctx->cell_n.p, ctx->prefix.p};
+        st = prepare(ctx, n, false, false);
+        if (st != TBMD_OK) return st;
+        void *after[4] = {ctx->state.p, ctx->nbr_buf.p, ctx->cell_n.p, ctx->prefix.p};
+        if (std::memcmp(before, after, sizeof before)) invalidate_graph(ctx);
+        CK(cudaMemsetAsync(ctx->scalars.as<char>() + 8, 0, 56, ctx->stream));
+        if (cut) {
+            CK(ctx->snapshot.ensure(sizeof(double) * 9 * (size_t)n));
+            CK(cudaMemcpyAsync(ctx->snapshot.p, ctx->s[0], sizeof(double) * 9 * n, cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+        }
+        if (ctx->cfg.use_graph && !ctx->profiling) {
+            if (!ctx->graph_valid) {
+                st = build_graph(ctx);
+                if (st != TBMD_OK) return st;
+            }
+            for (int it = 0; it < iterations; ++it) CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
+            ctx->launches += (uint64_t)ctx->graph_launches_per_step * iterations;
+        } else {
+            for (int it = 0; it < iterations; ++it) {
+                int nl = 0;
+                st = enqueue_step(ctx, ctx->stream, &nl);
+                if (st != TBMD_OK) return st;
+                ctx->launches += nl;
+            }
+        }
+        std::vector<unsigned long long> host(iterations);
+        int32_t seen = 0;
+        CK(cudaMemcpyAsync(host.data(), ctx->step_counts.p, sizeof(unsigned long long) * iterations,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(&seen, ctx->scalars.as<char>() + 28, sizeof seen, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        phase_resolve(ctx);
+        if (cut && grow_cap(ctx, seen)) {
+            CK(cudaMemcpyAsync(ctx->s[0], ctx->snapshot.p, sizeof(double) * 9 * n, cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+            continue;
+        }
+        if (counts)
+            for (int it = 0; it < iterations; ++it) counts[it] = host[it];
+        return TBMD_OK;
+    }
+    return fail(ctx, TBMD_CAPACITY_RETRY, "neighbour capacity still exceeded after retries (cap %d)", ctx->cap);
+}
+
+// Forward (dual = false) or adjoint (dual = true) evaluation with capacity retry, on ctx's state
+// or on caller device pointers.
+static tbmd_status evaluate(tbmd_ctx *ctx, int64_t n, Pos pos, Out out, bool dual, double *energy,
+                            unsigned long long *count, cudaStream_t st)
+{
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        tbmd_status s = prepare(ctx, n, dual, energy != nullptr);
+        if (s != TBMD_OK) return s;
+        CK(cudaMemsetAsync(ctx->scalars.as<char>() + 28, 0, 4, st));
+        if (energy) CK(cudaMemsetAsync(energy, 0, sizeof(double), st));
+        if (count) CK(cudaMemsetAsync(count, 0, sizeof(unsigned long long), st));
+        int nl = 0;
+        s = enqueue_forces(ctx, n, pos, out, dual, energy, count, st, &nl);
+        if (s != TBMD_OK) return s;
+        phase_mark(ctx, st, PH_END, nl);
+        ctx->launches += nl;
+        if (ctx->profiling) {
+            CK(cudaStreamSynchronize(st));
+            phase_resolve(ctx);
+        }
+        if (!is_p3bca_cut(ctx)) return TBMD_OK;
+        int32_t seen = 0;
+        CK(cudaMemcpyAsync(&seen, ctx->scalars.as<char>() + 28, sizeof seen, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (!grow_cap(ctx, seen)) return TBMD_OK;
+    }
+    return fail(ctx, TBMD_CAPACITY_RETRY, "neighbour capacity still exceeded after retries (cap %d)", ctx->cap);
+}
+
+tbmd_status tbmd_forces(tbmd_ctx *ctx, double *fx, double *fy, double *fz, double *energy, uint64_t *triplets)
+{
+    if (!ctx) return TBMD_INVALID_ARG;
+    if (ctx->n == 0) return fail(ctx, TBMD_NOT_READY, "no particles set");
+    tbmd_status st = check_device(ctx);
+    if (st != TBMD_OK) return st;
+    st = ensure_scalars(ctx);
+    if (st != TBMD_OK) return st;
+    st = evaluate(ctx, ctx->n, state_pos(ctx), state_out(ctx), false, energy_ptr(ctx), count_ptr(ctx), ctx->stream);
+    if (st != TBMD_OK) return st;
+    double e = 0;
+    unsigned long long c = 0;
+    const int64_t n = ctx->n;
+    if (fx) CK(cudaMemcpyAsync(fx, ctx->s[10], sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    if (fy) CK(cudaMemcpyAsync(fy, ctx->s[11], sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    if (fz) CK(cudaMemcpyAsync(fz, ctx->s[12], sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&e, energy_ptr(ctx), sizeof e, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&c, count_ptr(ctx), sizeof c, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (energy) *energy = e;
+    if (triplets) *triplets = c;
+    return TBMD_OK;
+}
+
+tbmd_status tbmd_forces_device(tbmd_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
+                               double *fx, double *fy, double *fz, double *energy, uint64_t *triplets, void *stream)
+{
+    if (!ctx || !x || !y || !z || !fx || !fy || !fz) return TBMD_INVALID_ARG;
+    if (n < 1) return fail(ctx, TBMD_INVALID_ARG, "n < 1");
+    tbmd_status st = check_device(ctx);
+    if (st != TBMD_OK) return st;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    return evaluate(ctx, n, Pos{x, y, z, nullptr, nullptr, nullptr}, Out{fx, fy, fz, nullptr, nullptr, nullptr}, false,
+                    energy, (unsigned long long *)triplets, s);
+}
+
+tbmd_status tbmd_adjoint_device(tbmd_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
+                                const double *gfx, const double *gfy, const double *gfz, const double *g_energy,
+                                double *fx, double *fy, double *fz, double *energy, double *gx, double *gy, double *gz,
+                                void *stream)
+{
+    (void)g_energy;
+    if (!ctx || !x || !y || !z || !gfx || !gfy || !gfz || !fx || !fy || !fz || !gx || !gy || !gz)
+        return TBMD_INVALID_ARG;
+    if (n < 1) return fail(ctx, TBMD_INVALID_ARG, "n < 1");
+    tbmd_status st = check_device(ctx);
+    if (st != TBMD_OK) return st;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    // gx receives H * gf; the caller adds g_energy * f (a device-side axpy it already owns).
+    return evaluate(ctx, n, Pos{x, y, z, gfx, gfy, gfz}, Out{fx, fy, fz, gx, gy, gz}, true, energy, nullptr, s);
+}
+
+tbmd_status tbmd_adjoint(tbmd_ctx *ctx, const double *gfx, const double *gfy, const double *gfz, double g_energy,
+                         double *gx, double *gy, double *gz, double *g_nu)
+{
+    if (!ctx || !gfx || !gfy || !gfz) return TBMD_INVALID_ARG;
+    if (ctx->n == 0) return fail(ctx, TBMD_NOT_READY, "no particles set");
+    if (!std::isfinite(g_energy)) return fail(ctx, TBMD_INVALID_ARG, "g_energy not finite");
+    tbmd_status st = check_device(ctx);
+    if (st != TBMD_OK) return st;
+    st = ensure_scalars(ctx);
+    if (st != TBMD_OK) return st;
+    const int64_t n = ctx->n;
+    CK(ctx->dirs.ensure(sizeof(double) * 3 * (size_t)n));
+    CK(ctx->hvp.ensure(sizeof(double) * 3 * (size_t)n));
+    double *d = ctx->dirs.as<double>(), *h = ctx->hvp.as<double>();
+    CK(cudaMemcpyAsync(d, gfx, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d + n, gfy, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d + 2 * n, gfz, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    const double nu = ctx->cfg.nu;
+    if (nu == 0.0) ctx->cfg.nu = 1.0;  // f and E are linear in nu: evaluate the nu = 1 parts
+    st = evaluate(ctx, n, Pos{ctx->s[0], ctx->s[1], ctx->s[2], d, d + n, d + 2 * n},
+                  Out{ctx->s[10], ctx->s[11], ctx->s[12], h, h + n, h + 2 * n}, true, energy_ptr(ctx), nullptr,
+                  ctx->stream);
+    ctx->cfg.nu = nu;
+    if (st != TBMD_OK) return st;
+    std::vector<double> f(3 * n), hv(3 * n);
+    double e = 0;
+    for (int k = 0; k < 3; ++k)
+        CK(cudaMemcpyAsync(f.data() + k * n, ctx->s[10 + k], sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(hv.data(), h, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&e, energy_ptr(ctx), sizeof e, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double scale = nu == 0.0 ? 0.0 : 1.0;  // with nu = 0 the true f, E and H are zero
+    const double *g3[3] = {gfx, gfy, gfz};
+    double *o3[3] = {gx, gy, gz};
+    double dot = 0.0;
+    for (int k = 0; k < 3; ++k)
+        for (int64_t i = 0; i < n; ++i) dot += g3[k][i] * f[k * n + i];
+    for (int k = 0; k < 3; ++k)
+        if (o3[k])
+            for (int64_t i = 0; i < n; ++i) o3[k][i] = scale * (hv[k * n + i] + g_energy * f[k * n + i]);
+    if (g_nu) *g_nu = nu == 0.0 ? dot + g_energy * e : (dot + g_energy * e) / nu;
+    if (nu == 0.0)  // leave the stored forces equal to the nu = 0 forces
+        for (int k = 0; k < 3; ++k) CK(cudaMemsetAsync(ctx->s[10 + k], 0, sizeof(double) * n, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TBMD_OK;
+}
+
+tbmd_status tbmd_cells(tbmd_ctx *ctx, int32_t *cell_of_particle, int32_t *dims, double *L, double *lo)
+{
+    if (!ctx) return TBMD_INVALID_ARG;
+    if (!ctx->domain_set) return fail(ctx, TBMD_NOT_READY, "no P3BCA domain");
+    if (!(ctx->cfg.cutoff > 0)) return fail(ctx, TBMD_INVALID_ARG, "no cutoff, no cell grid");
+    tbmd_status st = check_device(ctx);
+    if (st != TBMD_OK) return st;
+    make_grid(ctx);
+    if (dims)
+        for (int d = 0; d < 3; ++d) dims[d] = ctx->grid.dims[d];
+    if (L)
+        for (int d = 0; d < 3; ++d) L[d] = ctx->L[d];
+    if (lo)
+        for (int d = 0; d < 3; ++d) lo[d] = ctx->lo[d];
+    if (cell_of_particle) {
+        if (ctx->n == 0) return fail(ctx, TBMD_NOT_READY, "no particles set");
+        st = ensure_scalars(ctx);
+        if (st != TBMD_OK) return st;
+        st = ensure_cells(ctx, ctx->n, false, false);
+        if (st != TBMD_OK) return st;
+        int nl = 0;
+        CK(launch_cell_build(ctx->n, state_pos(ctx), ctx->grid, ctx->cb, false, ctx->stream, &nl));
+        ctx->launches += nl;
+        CK(cudaMemcpyAsync(cell_of_particle, ctx->cb.cell_of, sizeof(int32_t) * ctx->n, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return TBMD_OK;
+}
+
+tbmd_status tbmd_sync(tbmd_ctx *ctx)
+{
+    if (!ctx) return TBMD_INVALID_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TBMD_OK;
+}
+
+const char *tbmd_tuning(const tbmd_ctx *ctx) { return ctx ? ctx->tuning.c_str() : "{}"; }
+
+tbmd_status tbmd_set_profiling(tbmd_ctx *ctx, int32_t on)
+{
+    if (!ctx) return TBMD_INVALID_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    phase_resolve(ctx);
+    ctx->profiling = on != 0;
+    for (int k = 0; k < 5; ++k) {
+        ctx->phase_ms[k] = 0;
+        ctx->phase_calls[k] = 0;
+        ctx->phase_launches[k] = 0;
+    }
+    return TBMD_OK;
+}
+
+int32_t tbmd_phase_times(const tbmd_ctx *ctx, double *ms, uint64_t *calls, uint64_t *launches, int32_t max)
+{
+    if (!ctx) return 0;
+    int32_t k = max < 5 ? max : 5;
+    for (int32_t i = 0; i < k; ++i) {
+        if (ms) ms[i] = ctx->phase_ms[i];
+        if (calls) calls[i] = ctx->phase_calls[i];
+        if (launches) launches[i] = ctx->phase_launches[i];
+    }
+    return 5;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Autotuner: time each launch variant of the context's algorithm/precision at its current n on the
+// particle state (forces only), keep the fastest.  Cache: JSON Lines, one object per key
+// {"key": "<gpu>|<alg>|<prec>|n2^<bucket>", "R": r, "warps": w, "ms": t}.
+
+static std::string tune_key(tbmd_ctx *ctx)
+{
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, ctx->device);
+    int bucket = 0;
+    while ((int64_t(1) << (bucket + 1)) <= ctx->n) ++bucket;
+    char buf[400];
+    snprintf(buf, sizeof buf, "%s|%d|%d|cut%d|n2^%d", prop.name, ctx->cfg.algorithm, ctx->cfg.precision,
+             is_p3bca_cut(ctx) ? 1 : 0, bucket);
+    return buf;
+}
+
+static bool cache_lookup(const char *path, const std::string &key, int *R, int *warps)
+{
+    if (!path) return false;
+    FILE *f = fopen(path, "r");
+    if (!f) return false;
+    char line[1024];
+    bool found = false;
+    std::string needle = "\"key\": \"" + key + "\"";
+    while (fgets(line, sizeof line, f)) {
+        if (!strstr(line, needle.c_str())) continue;
+        const char *r = strstr(line, "\"R\": ");
+        const char *w = strstr(line, "\"warps\": ");
+        if (r && w) {
+            *R = atoi(r + 5);
+            *warps = atoi(w + 9);
+            found = true;
+        }
+    }
+    fclose(f);
+    return found;
+}
+
+static void cache_store(const char *path, const std::string &key, int R, int warps, float ms)
+{
+    if (!path) return;
+    FILE *f = fopen(path, "a");
+    if (!f) return;
+    fprintf(f, "{\"key\": \"%s\", \"R\": %d, \"warps\": %d, \"ms\": %.6f}\n", key.c_str(), R, warps, ms);
+    fclose(f);
+}
+
+static void apply_tuning(tbmd_ctx *ctx, int R, int warps)
+{
+    if (!mixed(ctx))
+        ctx->R_fp64 = R;
+    else if (ctx->cfg.algorithm == TBMD_NATA)
+        ctx->R_nata = R;
+    else
+        ctx->R_auta = R;
+    ctx->p3_warps = warps;
+    invalidate_graph(ctx);
+    char buf[160];
+    snprintf(buf, sizeof buf, "{\"R\": %d, \"warps\": %d}", sweep_R(ctx), ctx->p3_warps);
+    ctx->tuning = buf;
+}
+
+extern "C" tbmd_status tbmd_autotune(tbmd_ctx *ctx, const char *cache_path)
+{
+    if (!ctx) return TBMD_INVALID_ARG;
+    if (ctx->n == 0) return fail(ctx, TBMD_NOT_READY, "autotune needs particles");
+    tbmd_status st = check_device(ctx);
+    if (st != TBMD_OK) return st;
+    st = ensure_scalars(ctx);
+    if (st != TBMD_OK) return st;
+    const std::string key = tune_key(ctx);
+    int R = sweep_R(ctx), warps = ctx->p3_warps;
+    if (cache_lookup(cache_path, key, &R, &warps)) {
+        apply_tuning(ctx, R, warps);
+        return TBMD_OK;
+    }
+    std::vector<std::pair<int, int>> cand;
+    if (is_p3bca_cut(ctx)) {
+        for (int w : {2, 4, 8}) cand.push_back({R, w});
+    } else {
+        for (int r : {1, 2, 4}) cand.push_back({r, warps});
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    std::pair<int, int> arg = cand[0];
+    for (auto &c : cand) {
+        apply_tuning(ctx, c.first, c.second);
+        st = evaluate(ctx, ctx->n, state_pos(ctx), state_out(ctx), false, nullptr, nullptr, ctx->stream);  // warm-up
+        if (st != TBMD_OK) break;
+        CK(cudaEventRecord(e0, ctx->stream));
+        for (int rep = 0; rep < 3 && st == TBMD_OK; ++rep)
+            st = evaluate(ctx, ctx->n, state_pos(ctx), state_out(ctx), false, nullptr, nullptr, ctx->stream);
+        CK(cudaEventRecord(e1, ctx->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+            best = ms;
+            arg = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != TBMD_OK) return st;
+    apply_tuning(ctx, arg.first, arg.second);
+    cache_store(cache_path, key, arg.first, arg.second, best / 3);
+    return TBMD_OK;
+}
+
+extern "C" tbmd_status tbmd_batch_forces(tbmd_ctx *ctx, int32_t, const int64_t *, const double *, const double *,
+                                         const double *, const double *, const double *, double *, double *, double *,
+                                         double *, uint64_t *)
+{
+    return fail(ctx, TBMD_INVALID_ARG, "batched evaluation is not built yet");
+}
+
+extern "C" tbmd_status tbmd_batch_adjoint(tbmd_ctx *ctx, int32_t, const int64_t *, const double *, const double *,
+                                          const double *, const double *, const double *, const double *,
+                                          const double *, const double *, const double *, double *, double *, double *,
+                                          double *)
+{
+    return fail(ctx, TBMD_INVALID_ARG, "batched evaluation is not built yet");
+}

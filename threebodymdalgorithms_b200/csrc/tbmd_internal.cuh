@@ -1,0 +1,226 @@
+// Internal declarations shared by the kernels (tbmd_kernels.cu) and the C ABI (tbmd_api.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "at_math.cuh"
+
+namespace tbmd {
+
+// ---------------------------------------------------------------------------------------------
+// Scalar plumbing for the generic triplet kernels.  S is the arithmetic type of the triplet math:
+// double (FP64 drop-in), float (mixed precision), or Dual<double>/Dual<float> (the adjoint, whose
+// tangent part carries the Hessian-vector product).  Acc is the matching FP64 accumulator.
+
+template <class S>
+struct Traits;
+template <>
+struct Traits<double> {
+    using T = double;
+    using Acc = double;
+    static constexpr bool dual = false;
+};
+template <>
+struct Traits<float> {
+    using T = float;
+    using Acc = double;
+    static constexpr bool dual = false;
+};
+template <>
+struct Traits<Dual<double>> {
+    using T = double;
+    using Acc = Dual<double>;
+    static constexpr bool dual = true;
+};
+template <>
+struct Traits<Dual<float>> {
+    using T = float;
+    using Acc = Dual<double>;
+    static constexpr bool dual = true;
+};
+
+template <class S>
+struct V3 {
+    S x, y, z;
+};
+template <class S>
+__device__ __forceinline__ V3<S> operator+(V3<S> a, V3<S> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class S>
+__device__ __forceinline__ V3<S> operator-(V3<S> a, V3<S> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class S>
+__device__ __forceinline__ V3<S> operator*(V3<S> a, S s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class S>
+__device__ __forceinline__ S dot3(V3<S> a, V3<S> b) { return fma_(a.x, b.x, fma_(a.y, b.y, a.z * b.z)); }
+// acc + a * s, component-wise fused
+template <class S>
+__device__ __forceinline__ V3<S> fma3(V3<S> a, S s, V3<S> acc)
+{
+    return {fma_(a.x, s, acc.x), fma_(a.y, s, acc.y), fma_(a.z, s, acc.z)};
+}
+
+template <class S>
+__device__ __forceinline__ S szero() { return S(0); }
+template <>
+__device__ __forceinline__ Dual<double> szero<Dual<double>>() { return {0.0, 0.0}; }
+template <>
+__device__ __forceinline__ Dual<float> szero<Dual<float>>() { return {0.f, 0.f}; }
+template <class S>
+__device__ __forceinline__ V3<S> vzero() { return {szero<S>(), szero<S>(), szero<S>()}; }
+
+// A scalar of type S from an FP64 value and an FP64 tangent (ignored by non-dual types).
+template <class S>
+__device__ __forceinline__ S make_s(double v, double d);
+template <>
+__device__ __forceinline__ double make_s<double>(double v, double) { return v; }
+template <>
+__device__ __forceinline__ float make_s<float>(double v, double) { return (float)v; }
+template <>
+__device__ __forceinline__ Dual<double> make_s<Dual<double>>(double v, double d) { return {v, d}; }
+template <>
+__device__ __forceinline__ Dual<float> make_s<Dual<float>>(double v, double d) { return {(float)v, (float)d}; }
+
+template <class S>
+__device__ __forceinline__ S constant(double c) { return make_s<S>(c, 0.0); }
+
+// Widen to the FP64 accumulator type.
+__device__ __forceinline__ double to_acc(double v) { return v; }
+__device__ __forceinline__ double to_acc(float v) { return (double)v; }
+__device__ __forceinline__ Dual<double> to_acc(Dual<double> v) { return v; }
+__device__ __forceinline__ Dual<double> to_acc(Dual<float> v) { return {(double)v.v, (double)v.d}; }
+
+__device__ __forceinline__ double shfl_idx(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+__device__ __forceinline__ float shfl_idx(float v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+template <class T>
+__device__ __forceinline__ Dual<T> shfl_idx(Dual<T> v, int src)
+{
+    return {shfl_idx(v.v, src), shfl_idx(v.d, src)};
+}
+template <class S>
+__device__ __forceinline__ V3<S> shfl_idx(V3<S> v, int src)
+{
+    return {shfl_idx(v.x, src), shfl_idx(v.y, src), shfl_idx(v.z, src)};
+}
+__device__ __forceinline__ double shfl_xor_(double v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+template <class T>
+__device__ __forceinline__ Dual<T> shfl_xor_(Dual<T> v, int m)
+{
+    return {shfl_xor_(v.v, m), shfl_xor_(v.d, m)};
+}
+template <class A>
+__device__ __forceinline__ A warp_sum(A v)
+{
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) v = v + shfl_xor_(v, m);
+    return v;
+}
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
+{
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+    return v;
+}
+
+// Output of a triplet kernel: forces (the value part) and, for the adjoint, H * direction (the
+// tangent part), both accumulated in FP64.
+struct Out {
+    double *fx, *fy, *fz;
+    double *hx, *hy, *hz;
+};
+__device__ __forceinline__ void atomic_out(const Out &o, int64_t idx, V3<double> a)
+{
+    atomicAdd(o.fx + idx, a.x);
+    atomicAdd(o.fy + idx, a.y);
+    atomicAdd(o.fz + idx, a.z);
+}
+__device__ __forceinline__ void atomic_out(const Out &o, int64_t idx, V3<Dual<double>> a)
+{
+    atomicAdd(o.fx + idx, a.x.v);
+    atomicAdd(o.fy + idx, a.y.v);
+    atomicAdd(o.fz + idx, a.z.v);
+    atomicAdd(o.hx + idx, a.x.d);
+    atomicAdd(o.hy + idx, a.y.d);
+    atomicAdd(o.hz + idx, a.z.d);
+}
+__device__ __forceinline__ double acc_value(double a) { return a; }
+__device__ __forceinline__ double acc_value(Dual<double> a) { return a.v; }
+
+// ---------------------------------------------------------------------------------------------
+// Kernel argument blocks.
+
+// Positions (FP64 SoA) and, for the adjoint, the direction vector (cotangent on the forces).
+struct Pos {
+    const double *x, *y, *z;
+    const double *dx, *dy, *dz;
+};
+
+// Static work list of the no-cutoff sweeps.  A work item is (block b of JB consecutive j, i).
+struct SweepWork {
+    const int64_t *prefix;  // items of blocks < b, nblocks + 1 entries
+    int nblocks;
+    int64_t total;
+    unsigned int *counter;  // dynamic item counter, zeroed before the launch
+};
+
+// Cell grid of the P3BCA path.
+struct Grid {
+    double L[3], lo[3], w[3];
+    int dims[3];
+    int64_t ncells;
+    double sqcut;
+};
+
+// ---------------------------------------------------------------------------------------------
+// Launchers (tbmd_kernels.cu).  All take the stream they run on and return the launch error.
+
+int sweep_block_size(int algorithm, bool mixed, bool dual, int R);
+int64_t sweep_items(int algorithm, int64_t n, int JB, int64_t *prefix_host /* nb+1 or NULL */);
+
+cudaError_t launch_auta(bool mixed, bool dual, int R, bool energy, int64_t n, Pos pos, Out out, double *energy_out,
+                        double nu, SweepWork work, int grid, cudaStream_t st);
+cudaError_t launch_nata(bool mixed, bool dual, int R, bool energy, int64_t n, Pos pos, Out out, double *energy_out,
+                        double nu, SweepWork work, double *partial, int grid, cudaStream_t st);
+cudaError_t launch_nata_reduce(bool dual, int64_t n, int nblocks, const double *partial, Out out, cudaStream_t st);
+
+// P3BCA pipeline
+struct CellBufs {
+    int32_t *cell_of;      // [n] cell of each particle (input order)
+    int32_t *cell_count;   // [ncells]
+    int32_t *cell_start;   // [ncells + 1]
+    int32_t *cell_fill;    // [ncells]
+    int32_t *sorted;       // [n] sorted slot -> original index
+    double *xs, *ys, *zs;  // [n] positions in sorted order
+    double *dxs, *dys, *dzs;  // [n] adjoint direction in sorted order (or NULL)
+    int32_t *nbr;          // [n * cap] half neighbour lists (sorted indices)
+    int32_t *nbr_count;    // [n]
+    int32_t *max_count;    // [1] largest list length seen (overflow detection)
+    unsigned int *work_counter;  // [1] dynamic item counter of the triplet kernel
+    int cap;
+    double *fs[3];         // [n] forces in sorted order
+    double *hs[3];         // [n] H*direction in sorted order (adjoint)
+};
+cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, CellBufs &cb, bool with_dir, cudaStream_t st,
+                              int *launches);
+cudaError_t launch_neighbors(int64_t n, const Grid &g, CellBufs &cb, cudaStream_t st);
+// Launch shape of the P3BCA triplet kernel for a list capacity; computed outside graph capture.
+struct P3Plan {
+    int warps = 0;
+    size_t smem = 0;
+    int grid = 0;
+};
+cudaError_t plan_p3bca(bool mixed, bool dual, bool energy, int cap, int warps_requested, P3Plan *plan);
+cudaError_t launch_p3bca(bool mixed, bool dual, bool energy, int64_t n, const Grid &g, CellBufs &cb, double nu,
+                         double *energy_out, unsigned long long *count_out, const P3Plan &plan, cudaStream_t st);
+// forces (and H*d) from sorted order back to input order
+cudaError_t launch_unsort(int64_t n, const CellBufs &cb, Out out, bool dual, cudaStream_t st);
+
+// integrator
+cudaError_t launch_predictor(int64_t n, double *x, double *y, double *z, const double *vx, const double *vy,
+                             const double *vz, const double *ax, double dt, cudaStream_t st);
+cudaError_t launch_update(int64_t n, double *vx, double *vy, double *vz, double *ax, double *ay, double *az,
+                          const double *fx, const double *fy, const double *fz, const double *m, double dt, double gx,
+                          double gy, double gz, cudaStream_t st);
+cudaError_t launch_record_count(unsigned long long *cur, unsigned long long *per_step, unsigned int *step,
+                                unsigned long long constant_count, cudaStream_t st);
+
+}  // namespace tbmd

@@ -1,0 +1,836 @@
+// CUDA kernels (sm_100a) of the Axilrod-Teller three-body path.
+//
+//   k_auta       AUTA: every unique triplet i < j < k once (Algorithm.cpp:72-141 with one owner).
+//                A warp takes a work item (block of 32*R consecutive j, one i): lanes own the j
+//                (register accumulators), k sweeps the rest of the system in tiles of 32 staged in
+//                shared memory.  The k-side contributions travel with a rotating accumulator (one
+//                shuffle per tile step) so that after 32 steps lane l holds the complete sum for
+//                k = tile + l and writes it with one FP64 atomic.  i's force is -(sum of the j- and
+//                k-side totals) by translation invariance, so it costs nothing per triplet.
+//   k_nata       NATA: all triplets seen from each particle i; only grad_i is accumulated, no
+//                atomics; per-(i, j-block) partial sums are reduced in a fixed order (deterministic).
+//   k_cell_*     P3BCA cell grid: wrap-and-bin (FP64, same arithmetic as the oracle), counting sort
+//                by cell, stable within a cell.
+//   k_neighbors  half neighbour lists (sorted index t > s) with the reference's exact FP64
+//                periodic cutoff test (structs.hpp:106-115; d == cutoff is inside).
+//   k_p3bca      warp per particle s: all pairs (a < b) of its half list, exact FP64 test of the
+//                third edge, triplet math, per-slot accumulation in shared memory, one FP64 atomic
+//                per list slot.
+//   k_predictor / k_update   the reference's integrator (structs.hpp:40-99), FP64.
+//
+// Precision: S = double is the FP64 drop-in.  S = float is the mixed form: displacements are
+// formed in FP64 from FP64 positions and rounded once (relative to particle i, so they are small
+// and accurate), the triplet geometry and coefficients are FP32, short FP32 partial sums (at
+// most one 32-wide tile) are flushed into FP64 accumulators, and all global accumulation is FP64.
+// S = Dual<T> is the adjoint: the same kernels carry a tangent (the cotangent on the forces as a
+// direction) and return H * direction alongside the forces.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "tbmd_internal.cuh"
+
+namespace tbmd {
+
+template <class S>
+struct Tile {
+    S vx, vy, vz, b;
+};
+
+template <class S>
+__device__ __forceinline__ V3<typename Traits<S>::Acc> widen(V3<S> a)
+{
+    return {to_acc(a.x), to_acc(a.y), to_acc(a.z)};
+}
+
+template <class A>
+__device__ __forceinline__ V3<A> warp_sum3(V3<A> v)
+{
+    return {warp_sum(v.x), warp_sum(v.y), warp_sum(v.z)};
+}
+
+// Displacement x_j - x_i as S: FP64 subtraction, then one rounding; the tangent carries d_j - d_i.
+template <class S>
+__device__ __forceinline__ V3<S> disp(const Pos &p, int64_t j, double xi, double yi, double zi, double dxi,
+                                      double dyi, double dzi)
+{
+    if (Traits<S>::dual)
+        return {make_s<S>(p.x[j] - xi, p.dx[j] - dxi), make_s<S>(p.y[j] - yi, p.dy[j] - dyi),
+                make_s<S>(p.z[j] - zi, p.dz[j] - dzi)};
+    return {make_s<S>(p.x[j] - xi, 0.0), make_s<S>(p.y[j] - yi, 0.0), make_s<S>(p.z[j] - zi, 0.0)};
+}
+
+// Decode a sweep work item: block b with prefix[b] <= w < prefix[b+1], i = w - prefix[b].
+__device__ __forceinline__ int find_block(const int64_t *prefix, int nblocks, int64_t w)
+{
+    int lo = 0, hi = nblocks;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(prefix + mid) <= w)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------------------------
+// AUTA sweep
+
+template <class S, int R, bool ENERGY, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out, double *energy_out, double nu_d,
+                                                    SweepWork work)
+{
+    using Acc = typename Traits<S>::Acc;
+    constexpr int JB = 32 * R;
+    __shared__ Tile<S> tile[WARPS][32];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const S nu = constant<S>(nu_d), nu3 = constant<S>(-3.0 * nu_d), nu15 = constant<S>(15.0 * nu_d);
+    Acc en_acc = to_acc(szero<S>());
+
+    unsigned int w = 0;
+    if (lane == 0) w = atomicAdd(work.counter, 1u);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    while ((int64_t)w < work.total) {
+        unsigned int wn = 0;
+        if (lane == 0) wn = atomicAdd(work.counter, 1u);
+        const int b = find_block(work.prefix, work.nblocks, (int64_t)w);
+        const int64_t i = (int64_t)w - work.prefix[b];
+        const double xi = pos.x[i], yi = pos.y[i], zi = pos.z[i];
+        double dxi = 0.0, dyi = 0.0, dzi = 0.0;
+        if (Traits<S>::dual) {
+            dxi = pos.dx[i];
+            dyi = pos.dy[i];
+            dzi = pos.dz[i];
+        }
+        V3<S> u[R];
+        S aa[R];
+        int64_t jj[R];
+        bool jv[R];
+        V3<Acc> fj[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            jj[r] = (int64_t)b * JB + r * 32 + lane;
+            jv[r] = jj[r] > i && jj[r] < n;
+            u[r] = jv[r] ? disp<S>(pos, jj[r], xi, yi, zi, dxi, dyi, dzi) : vzero<S>();
+            aa[r] = dot3(u[r], u[r]);
+            fj[r] = widen(vzero<S>());
+        }
+        V3<Acc> fi = widen(vzero<S>());
+        for (int64_t kt = (int64_t)b * JB; kt < n; kt += 32) {
+            const int64_t k = kt + lane;
+            const bool kv = k < n;
+            const V3<S> vk = kv ? disp<S>(pos, k, xi, yi, zi, dxi, dyi, dzi) : vzero<S>();
+            tile[wib][lane] = {vk.x, vk.y, vk.z, dot3(vk, vk)};
+            __syncwarp();
+            S al[R];
+            V3<S> gv[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                al[r] = szero<S>();
+                gv[r] = vzero<S>();
+            }
+            S bsum = szero<S>();
+            V3<S> gus = vzero<S>();
+            S en = szero<S>();
+#pragma unroll 2
+            for (int t = 0; t < 32; ++t) {
+                const int kk = (lane + t) & 31;
+                const Tile<S> e = tile[wib][kk];
+                const V3<S> v = {e.vx, e.vy, e.vz};
+                const int64_t kidx = kt + kk;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const bool valid = jv[r] && kidx > jj[r] && kidx < n;
+                    const S p = dot3(u[r], v);
+                    const ATCoef<S> cf = at_coef<ENERGY>(aa[r], e.b, p, nu, nu3, nu15, valid, en);
+                    al[r] = al[r] + cf.alpha;
+                    gv[r] = fma3(v, cf.gamma, gv[r]);
+                    bsum = bsum + cf.beta;
+                    gus = fma3(u[r], cf.gamma, gus);
+                }
+                const int src = (lane + 1) & 31;
+                bsum = shfl_idx(bsum, src);
+                gus = shfl_idx(gus, src);
+            }
+            // After the full rotation lane l holds the k-side sums of k = kt + l.
+            const V3<Acc> fk = widen(fma3(vk, bsum, gus));
+            if (kv) atomic_out(out, k, fk);
+            fi = fi - fk;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const V3<Acc> f = widen(fma3(u[r], al[r], gv[r]));
+                fj[r] = fj[r] + f;
+                fi = fi - f;
+            }
+            if (ENERGY) en_acc = en_acc + to_acc(en);
+            __syncwarp();
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (jv[r]) atomic_out(out, jj[r], fj[r]);
+        fi = warp_sum3(fi);
+        if (lane == 0) atomic_out(out, i, fi);
+        w = __shfl_sync(0xffffffffu, wn, 0);
+    }
+    if (ENERGY) {
+        en_acc = warp_sum(en_acc);
+        if (lane == 0) atomicAdd(energy_out, acc_value(en_acc));
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// NATA sweep: item (j-block b, particle i) sums grad_i over all pairs j < k (j in block b, both
+// different from i).  Energy is counted only for i < j < k, so each triplet's energy once.
+
+template <class S, int R, bool ENERGY, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_nata(int64_t n, Pos pos, double *partial, double *energy_out,
+                                                    double nu_d, SweepWork work)
+{
+    using Acc = typename Traits<S>::Acc;
+    constexpr int JB = 32 * R;
+    __shared__ Tile<S> tile[WARPS][32];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const S nu = constant<S>(nu_d), nu3 = constant<S>(-3.0 * nu_d), nu15 = constant<S>(15.0 * nu_d);
+    Acc en_acc = to_acc(szero<S>());
+    const int nb = work.nblocks;
+
+    unsigned int w = 0;
+    if (lane == 0) w = atomicAdd(work.counter, 1u);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    while ((int64_t)w < work.total) {
+        unsigned int wn = 0;
+        if (lane == 0) wn = atomicAdd(work.counter, 1u);
+        const int b = (int)((int64_t)w / n);
+        const int64_t i = (int64_t)w - (int64_t)b * n;
+        const double xi = pos.x[i], yi = pos.y[i], zi = pos.z[i];
+        V3<S> u[R];
+        S aa[R];
+        int64_t jj[R];
+        bool jv[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            jj[r] = (int64_t)b * JB + r * 32 + lane;
+            jv[r] = jj[r] < n && jj[r] != i;
+            u[r] = jv[r] ? disp<S>(pos, jj[r], xi, yi, zi, 0.0, 0.0, 0.0) : vzero<S>();
+            aa[r] = dot3(u[r], u[r]);
+        }
+        V3<Acc> g = widen(vzero<S>());
+        for (int64_t kt = (int64_t)b * JB; kt < n; kt += 32) {
+            const int64_t k = kt + lane;
+            const V3<S> vk = (k < n) ? disp<S>(pos, k, xi, yi, zi, 0.0, 0.0, 0.0) : vzero<S>();
+            tile[wib][lane] = {vk.x, vk.y, vk.z, dot3(vk, vk)};
+            __syncwarp();
+            S A[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) A[r] = szero<S>();
+            V3<S> Bv = vzero<S>();
+            S en = szero<S>();
+#pragma unroll 2
+            for (int t = 0; t < 32; ++t) {
+                const Tile<S> e = tile[wib][t];
+                const V3<S> v = {e.vx, e.vy, e.vz};
+                const int64_t kidx = kt + t;
+                const bool kv = kidx < n && kidx != i;
+                S bs = szero<S>();
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const bool valid = jv[r] && kv && kidx > jj[r];
+                    const S p = dot3(u[r], v);
+                    S e_r = szero<S>();
+                    const ATCoef<S> cf = at_coef<ENERGY>(aa[r], e.b, p, nu, nu3, nu15, valid, e_r);
+                    if (ENERGY && i < jj[r]) en = en + e_r;
+                    A[r] = A[r] + (cf.alpha + cf.gamma);
+                    bs = bs + (cf.beta + cf.gamma);
+                }
+                Bv = fma3(v, bs, Bv);
+            }
+            V3<S> gt = Bv;
+#pragma unroll
+            for (int r = 0; r < R; ++r) gt = fma3(u[r], A[r], gt);
+            g = g + widen(gt);
+            if (ENERGY) en_acc = en_acc + to_acc(en);
+            __syncwarp();
+        }
+        g = warp_sum3(g);
+        if (lane == 0) {
+            double *dst = partial + ((int64_t)i * nb + b) * 3;
+            dst[0] = -acc_value(g.x);
+            dst[1] = -acc_value(g.y);
+            dst[2] = -acc_value(g.z);
+        }
+        w = __shfl_sync(0xffffffffu, wn, 0);
+    }
+    if (ENERGY) {
+        en_acc = warp_sum(en_acc);
+        if (lane == 0) atomicAdd(energy_out, acc_value(en_acc));
+    }
+}
+
+// f_i = sum over blocks b of partial[i][b], in block order.
+__global__ void k_nata_reduce(int64_t n, int nb, const double *__restrict__ partial, Out out)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    const double *p = partial + i * nb * 3;
+    for (int b = 0; b < nb; ++b) {
+        sx += p[3 * b + 0];
+        sy += p[3 * b + 1];
+        sz += p[3 * b + 2];
+    }
+    out.fx[i] = sx;
+    out.fy[i] = sy;
+    out.fz[i] = sz;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Work lists and launch helpers for the sweeps.
+
+constexpr int SWEEP_WARPS = 8;
+
+int64_t sweep_items(int algorithm, int64_t n, int JB, int64_t *prefix)
+{
+    // AUTA (algorithm 2): block b = [b*JB, (b+1)*JB) needs j <= n-2 and i < j, so it has
+    // min((b+1)*JB - 1, n - 2) items i = 0 ..; NATA (0): every block with j <= n-2 pairs with all n i.
+    int64_t nb = n >= 3 ? (n - 2 + JB) / JB : 0;  // blocks holding some j <= n - 2
+    int64_t total = 0;
+    if (prefix) prefix[0] = 0;
+    for (int64_t b = 0; b < nb; ++b) {
+        int64_t cnt = algorithm == 0 ? n : std::min<int64_t>((b + 1) * JB - 1, n - 2);
+        if (cnt < 0) cnt = 0;
+        total += cnt;
+        if (prefix) prefix[b + 1] = total;
+    }
+    return total;
+}
+
+int sweep_block_size(int, bool, bool, int) { return SWEEP_WARPS * 32; }
+
+template <class S, int R>
+static cudaError_t launch_auta_t(bool energy, int64_t n, Pos pos, Out out, double *eo, double nu, SweepWork work,
+                                 int grid, cudaStream_t st)
+{
+    if (work.total <= 0) return cudaSuccess;
+    if (energy)
+        k_auta<S, R, true, SWEEP_WARPS><<<grid, SWEEP_WARPS * 32, 0, st>>>(n, pos, out, eo, nu, work);
+    else
+        k_auta<S, R, false, SWEEP_WARPS><<<grid, SWEEP_WARPS * 32, 0, st>>>(n, pos, out, eo, nu, work);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_auta(bool mixed, bool dual, int R, bool energy, int64_t n, Pos pos, Out out, double *eo, double nu,
+                        SweepWork work, int grid, cudaStream_t st)
+{
+    if (dual) {
+        if (mixed) return launch_auta_t<Dual<float>, 2>(energy, n, pos, out, eo, nu, work, grid, st);
+        return launch_auta_t<Dual<double>, 1>(energy, n, pos, out, eo, nu, work, grid, st);
+    }
+    if (mixed) {
+        switch (R) {
+            case 1: return launch_auta_t<float, 1>(energy, n, pos, out, eo, nu, work, grid, st);
+            case 2: return launch_auta_t<float, 2>(energy, n, pos, out, eo, nu, work, grid, st);
+            default: return launch_auta_t<float, 4>(energy, n, pos, out, eo, nu, work, grid, st);
+        }
+    }
+    switch (R) {
+        case 1: return launch_auta_t<double, 1>(energy, n, pos, out, eo, nu, work, grid, st);
+        case 4: return launch_auta_t<double, 4>(energy, n, pos, out, eo, nu, work, grid, st);
+        default: return launch_auta_t<double, 2>(energy, n, pos, out, eo, nu, work, grid, st);
+    }
+}
+
+template <class S, int R>
+static cudaError_t launch_nata_t(bool energy, int64_t n, Pos pos, double *partial, double *eo, double nu,
+                                 SweepWork work, int grid, cudaStream_t st)
+{
+    if (work.total <= 0) return cudaSuccess;
+    if (energy)
+        k_nata<S, R, true, SWEEP_WARPS><<<grid, SWEEP_WARPS * 32, 0, st>>>(n, pos, partial, eo, nu, work);
+    else
+        k_nata<S, R, false, SWEEP_WARPS><<<grid, SWEEP_WARPS * 32, 0, st>>>(n, pos, partial, eo, nu, work);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_nata(bool mixed, bool dual, int R, bool energy, int64_t n, Pos pos, Out, double *eo, double nu,
+                        SweepWork work, double *partial, int grid, cudaStream_t st)
+{
+    if (dual) return cudaErrorInvalidValue;  // the adjoint of NATA uses the AUTA sweep (same triplet set)
+    if (mixed) {
+        switch (R) {
+            case 1: return launch_nata_t<float, 1>(energy, n, pos, partial, eo, nu, work, grid, st);
+            case 2: return launch_nata_t<float, 2>(energy, n, pos, partial, eo, nu, work, grid, st);
+            default: return launch_nata_t<float, 4>(energy, n, pos, partial, eo, nu, work, grid, st);
+        }
+    }
+    switch (R) {
+        case 1: return launch_nata_t<double, 1>(energy, n, pos, partial, eo, nu, work, grid, st);
+        case 4: return launch_nata_t<double, 4>(energy, n, pos, partial, eo, nu, work, grid, st);
+        default: return launch_nata_t<double, 2>(energy, n, pos, partial, eo, nu, work, grid, st);
+    }
+}
+
+cudaError_t launch_nata_reduce(bool, int64_t n, int nblocks, const double *partial, Out out, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    k_nata_reduce<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, nblocks, partial, out);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------
+// P3BCA cell grid.  Arithmetic without FMA contraction so that it equals the oracle's C code.
+
+__device__ __forceinline__ int cell_coord(double x, double lo, double w, int nd)
+{
+    double t = floor(__ddiv_rn(__dsub_rn(x, lo), w));
+    double m = fmod(t, (double)nd);
+    if (m < 0) m = __dadd_rn(m, (double)nd);
+    int c = (int)m;
+    return c >= nd ? nd - 1 : c;
+}
+
+// Particle::GetSqrDistPeriodic (structs.hpp:106-115), evaluated in the reference's order.
+__device__ __forceinline__ double sqdist_periodic(double xa, double ya, double za, double xb, double yb, double zb,
+                                                  const Grid &g)
+{
+    double ax = fabs(__dsub_rn(xb, xa)), ay = fabs(__dsub_rn(yb, ya)), az = fabs(__dsub_rn(zb, za));
+    double mx = fmin(ax, __dsub_rn(g.L[0], ax)), my = fmin(ay, __dsub_rn(g.L[1], ay)),
+           mz = fmin(az, __dsub_rn(g.L[2], az));
+    return __dadd_rn(__dadd_rn(__dmul_rn(mx, mx), __dmul_rn(my, my)), __dmul_rn(mz, mz));
+}
+
+__global__ void k_cell_assign(int64_t n, const double *__restrict__ x, const double *__restrict__ y,
+                              const double *__restrict__ z, Grid g, int32_t *__restrict__ cell_of,
+                              int32_t *__restrict__ cell_count)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int cx = cell_coord(x[i], g.lo[0], g.w[0], g.dims[0]);
+    int cy = cell_coord(y[i], g.lo[1], g.w[1], g.dims[1]);
+    int cz = cell_coord(z[i], g.lo[2], g.w[2], g.dims[2]);
+    int c = (cz * g.dims[1] + cy) * g.dims[0] + cx;
+    cell_of[i] = c;
+    atomicAdd(cell_count + c, 1);
+}
+
+// Exclusive scan of cell counts (single block of 1024 threads, each owning a contiguous chunk).
+__global__ void __launch_bounds__(1024) k_cell_scan(int64_t ncells, const int32_t *__restrict__ count,
+                                                    int32_t *__restrict__ start)
+{
+    __shared__ int32_t part[1024];
+    const int t = threadIdx.x;
+    const int64_t chunk = (ncells + 1023) / 1024;
+    const int64_t b = t * chunk, e = (b + chunk < ncells) ? b + chunk : ncells;
+    int32_t s = 0;
+    for (int64_t c = b; c < e; ++c) s += count[c];
+    part[t] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        int32_t v = t >= off ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int32_t run = part[t] - s;
+    for (int64_t c = b; c < e; ++c) {
+        start[c] = run;
+        run += count[c];
+    }
+    if (t == 1023) start[ncells] = part[1023];
+}
+
+__global__ void k_cell_scatter(int64_t n, const int32_t *__restrict__ cell_of, const int32_t *__restrict__ start,
+                               int32_t *__restrict__ fill, int32_t *__restrict__ sorted)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c = cell_of[i];
+    int slot = atomicAdd(fill + c, 1);
+    sorted[start[c] + slot] = (int32_t)i;
+}
+
+// Order each cell's members by original index (insertion sort; cells hold tens of particles),
+// then gather positions (and the adjoint direction) into sorted order.
+__global__ void k_cell_order(int64_t ncells, const int32_t *__restrict__ start, int32_t *__restrict__ sorted)
+{
+    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    int32_t b = start[c], e = start[c + 1];
+    for (int32_t p = b + 1; p < e; ++p) {
+        int32_t v = sorted[p], q = p - 1;
+        while (q >= b && sorted[q] > v) {
+            sorted[q + 1] = sorted[q];
+            --q;
+        }
+        sorted[q + 1] = v;
+    }
+}
+
+__global__ void k_gather(int64_t n, const int32_t *__restrict__ sorted, Pos pos, double *xs, double *ys, double *zs,
+                         double *dxs, double *dys, double *dzs)
+{
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    int32_t i = sorted[s];
+    xs[s] = pos.x[i];
+    ys[s] = pos.y[i];
+    zs[s] = pos.z[i];
+    if (dxs) {
+        dxs[s] = pos.dx[i];
+        dys[s] = pos.dy[i];
+        dzs[s] = pos.dz[i];
+    }
+}
+
+cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, CellBufs &cb, bool with_dir, cudaStream_t st,
+                              int *launches)
+{
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    const unsigned cb_blocks = (unsigned)((g.ncells + 255) / 256);
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(cb.cell_count, 0, sizeof(int32_t) * g.ncells, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(cb.cell_fill, 0, sizeof(int32_t) * g.ncells, st)) != cudaSuccess) return e;
+    k_cell_assign<<<nb, 256, 0, st>>>(n, pos.x, pos.y, pos.z, g, cb.cell_of, cb.cell_count);
+    k_cell_scan<<<1, 1024, 0, st>>>(g.ncells, cb.cell_count, cb.cell_start);
+    k_cell_scatter<<<nb, 256, 0, st>>>(n, cb.cell_of, cb.cell_start, cb.cell_fill, cb.sorted);
+    k_cell_order<<<cb_blocks, 256, 0, st>>>(g.ncells, cb.cell_start, cb.sorted);
+    k_gather<<<nb, 256, 0, st>>>(n, cb.sorted, pos, cb.xs, cb.ys, cb.zs, with_dir ? cb.dxs : nullptr,
+                                 with_dir ? cb.dys : nullptr, with_dir ? cb.dzs : nullptr);
+    if (launches) *launches += 5;
+    return cudaGetLastError();
+}
+
+// Half neighbour lists: for sorted particle s, every t > s in the 27 (fewer on one-cell axes)
+// neighbouring cells with periodic d^2 <= cutoff^2.  Lists longer than cap are truncated; the
+// largest length is recorded so the host can enlarge cap and recompute.
+__global__ void k_neighbors(int64_t n, Grid g, const double *__restrict__ xs, const double *__restrict__ ys,
+                            const double *__restrict__ zs, const int32_t *__restrict__ cell_start, int32_t *nbr,
+                            int32_t *nbr_count, int32_t *max_count, int cap)
+{
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const double xa = xs[s], ya = ys[s], za = zs[s];
+    const int cx = cell_coord(xa, g.lo[0], g.w[0], g.dims[0]);
+    const int cy = cell_coord(ya, g.lo[1], g.w[1], g.dims[1]);
+    const int cz = cell_coord(za, g.lo[2], g.w[2], g.dims[2]);
+    int cnt = 0;
+    int32_t *dst = nbr + s * (int64_t)cap;
+    const int lz = g.dims[2] == 1 ? 0 : -1, hz = g.dims[2] == 1 ? 0 : 1;
+    const int ly = g.dims[1] == 1 ? 0 : -1, hy = g.dims[1] == 1 ? 0 : 1;
+    const int lx = g.dims[0] == 1 ? 0 : -1, hx = g.dims[0] == 1 ? 0 : 1;
+    for (int oz = lz; oz <= hz; ++oz) {
+        const int nz = (cz + oz + g.dims[2]) % g.dims[2];
+        for (int oy = ly; oy <= hy; ++oy) {
+            const int ny = (cy + oy + g.dims[1]) % g.dims[1];
+            for (int ox = lx; ox <= hx; ++ox) {
+                const int nx = (cx + ox + g.dims[0]) % g.dims[0];
+                const int nc = (nz * g.dims[1] + ny) * g.dims[0] + nx;
+                const int32_t e = cell_start[nc + 1];
+                for (int32_t t = max(cell_start[nc], (int32_t)s + 1); t < e; ++t) {
+                    if (sqdist_periodic(xa, ya, za, xs[t], ys[t], zs[t], g) > g.sqcut) continue;
+                    if (cnt < cap) dst[cnt] = t;
+                    ++cnt;
+                }
+            }
+        }
+    }
+    nbr_count[s] = cnt;
+    atomicMax(max_count, cnt);
+}
+
+cudaError_t launch_neighbors(int64_t n, const Grid &g, CellBufs &cb, cudaStream_t st)
+{
+    k_neighbors<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, g, cb.xs, cb.ys, cb.zs, cb.cell_start, cb.nbr,
+                                                            cb.nbr_count, cb.max_count, cb.cap);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------
+// P3BCA triplets.  Warp per sorted particle s (dynamic item counter).  The half list (a slot per
+// neighbour) is staged in the warp's shared memory: displacement from s as S and its square,
+// the FP64 position for the exact third-edge test, and an S accumulator per slot.  Lanes walk the
+// flattened list of slot pairs (a < b); each inside triplet adds its j- and k-side gradient into
+// the slot accumulators (shared atomics) and its i-side into a register.  At the end every slot
+// is flushed with one FP64 atomic.
+
+template <class S>
+__device__ __forceinline__ void satomic_add(S *p, S v)
+{
+    atomicAdd(p, v);
+}
+template <>
+__device__ __forceinline__ void satomic_add<Dual<double>>(Dual<double> *p, Dual<double> v)
+{
+    atomicAdd(&p->v, v.v);
+    atomicAdd(&p->d, v.d);
+}
+template <>
+__device__ __forceinline__ void satomic_add<Dual<float>>(Dual<float> *p, Dual<float> v)
+{
+    atomicAdd(&p->v, v.v);
+    atomicAdd(&p->d, v.d);
+}
+
+template <class S>
+struct SlotLayout {
+    // per-warp shared memory: [cap] of each
+    static constexpr size_t bytes_per_slot = 4 * sizeof(S) + 3 * sizeof(double) + 3 * sizeof(S) + sizeof(int32_t);
+};
+
+template <class S, bool ENERGY>
+__global__ void k_p3bca(int64_t n, Grid g, CellBufs cb, double nu_d, double *energy_out,
+                        unsigned long long *count_out, unsigned int *counter)
+{
+    using Acc = typename Traits<S>::Acc;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int cap = cb.cap;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    unsigned char *base = smem + (size_t)wib * cap * SlotLayout<S>::bytes_per_slot;
+    double *px = (double *)base;
+    double *py = px + cap;
+    double *pz = py + cap;
+    S *vx = (S *)(pz + cap);
+    S *vy = vx + cap;
+    S *vz = vy + cap;
+    S *vb = vz + cap;
+    S *gx = vb + cap;
+    S *gy = gx + cap;
+    S *gz = gy + cap;
+    int32_t *idx = (int32_t *)(gz + cap);
+
+    const S nu = constant<S>(nu_d), nu3 = constant<S>(-3.0 * nu_d), nu15 = constant<S>(15.0 * nu_d);
+    const Out outs = {cb.fs[0], cb.fs[1], cb.fs[2], cb.hs[0], cb.hs[1], cb.hs[2]};
+    const bool dual = Traits<S>::dual;
+    unsigned long long cnt = 0;
+    Acc en_acc = to_acc(szero<S>());
+
+    unsigned int w = 0;
+    if (lane == 0) w = atomicAdd(counter, 1u);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    while ((int64_t)w < n) {
+        unsigned int wn = 0;
+        if (lane == 0) wn = atomicAdd(counter, 1u);
+        const int64_t s = w;
+        const int M = min(cb.nbr_count[s], cap);
+        const double xi = cb.xs[s], yi = cb.ys[s], zi = cb.zs[s];
+        const double dxi = dual ? cb.dxs[s] : 0.0, dyi = dual ? cb.dys[s] : 0.0, dzi = dual ? cb.dzs[s] : 0.0;
+        for (int e = lane; e < M; e += 32) {
+            const int32_t t = cb.nbr[s * (int64_t)cap + e];
+            idx[e] = t;
+            const double x = cb.xs[t], y = cb.ys[t], z = cb.zs[t];
+            px[e] = x;
+            py[e] = y;
+            pz[e] = z;
+            V3<S> v = {make_s<S>(x - xi, dual ? cb.dxs[t] - dxi : 0.0), make_s<S>(y - yi, dual ? cb.dys[t] - dyi : 0.0),
+                       make_s<S>(z - zi, dual ? cb.dzs[t] - dzi : 0.0)};
+            vx[e] = v.x;
+            vy[e] = v.y;
+            vz[e] = v.z;
+            vb[e] = dot3(v, v);
+            gx[e] = szero<S>();
+            gy[e] = szero<S>();
+            gz[e] = szero<S>();
+        }
+        __syncwarp();
+        const int64_t P = (int64_t)M * (M - 1) / 2;
+        // pair index p = bb*(bb-1)/2 + a with a < bb
+        int64_t p = lane;
+        int bb = (int)((1.0 + sqrt(1.0 + 8.0 * (double)p)) * 0.5);
+        while ((int64_t)bb * (bb - 1) / 2 > p) --bb;
+        while ((int64_t)(bb + 1) * bb / 2 <= p) ++bb;
+        int a = (int)(p - (int64_t)bb * (bb - 1) / 2);
+        V3<S> gi = vzero<S>();
+        S en = szero<S>();
+        for (; p < P; p += 32) {
+            if (sqdist_periodic(px[a], py[a], pz[a], px[bb], py[bb], pz[bb], g) <= g.sqcut) {
+                ++cnt;
+                const V3<S> u = {vx[a], vy[a], vz[a]};
+                const V3<S> v = {vx[bb], vy[bb], vz[bb]};
+                const S pp = dot3(u, v);
+                const ATCoef<S> cf = at_coef<ENERGY>(vb[a], vb[bb], pp, nu, nu3, nu15, true, en);
+                const V3<S> ga = fma3(u, cf.alpha, v * cf.gamma);
+                const V3<S> gb = fma3(v, cf.beta, u * cf.gamma);
+                satomic_add(gx + a, ga.x);
+                satomic_add(gy + a, ga.y);
+                satomic_add(gz + a, ga.z);
+                satomic_add(gx + bb, gb.x);
+                satomic_add(gy + bb, gb.y);
+                satomic_add(gz + bb, gb.z);
+                gi = gi + ga + gb;
+            }
+            a += 32;
+            while (a >= bb) {
+                a -= bb;
+                ++bb;
+            }
+        }
+        __syncwarp();
+        for (int e = lane; e < M; e += 32) atomic_out(outs, idx[e], widen(V3<S>{gx[e], gy[e], gz[e]}));
+        V3<Acc> gia = warp_sum3(widen(gi));
+        if (lane == 0) atomic_out(outs, s, V3<Acc>{-gia.x, -gia.y, -gia.z});
+        if (ENERGY) en_acc = en_acc + to_acc(en);
+        __syncwarp();
+        w = __shfl_sync(0xffffffffu, wn, 0);
+    }
+    cnt = warp_sum_u64(cnt);
+    if (lane == 0 && count_out) atomicAdd(count_out, cnt);
+    if (ENERGY) {
+        en_acc = warp_sum(en_acc);
+        if (lane == 0) atomicAdd(energy_out, acc_value(en_acc));
+    }
+}
+
+template <class S>
+static cudaError_t plan_p3bca_t(bool energy, int cap, int warps, P3Plan *plan)
+{
+    int dev = 0, num_sms = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    const size_t per_warp = (size_t)cap * SlotLayout<S>::bytes_per_slot;
+    const size_t smem_cap = 200 * 1024;
+    if (warps < 1) warps = 1;
+    while (warps > 1 && per_warp * warps > smem_cap) --warps;
+    if (per_warp * warps > smem_cap) return cudaErrorInvalidValue;
+    const size_t smem = per_warp * warps;
+    auto kern = energy ? k_p3bca<S, true> : k_p3bca<S, false>;
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+        return e;
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem)) != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    plan->warps = warps;
+    plan->smem = smem;
+    plan->grid = num_sms * per_sm;
+    return cudaSuccess;
+}
+
+cudaError_t plan_p3bca(bool mixed, bool dual, bool energy, int cap, int warps, P3Plan *plan)
+{
+    if (dual) {
+        if (mixed) return plan_p3bca_t<Dual<float>>(energy, cap, warps, plan);
+        return plan_p3bca_t<Dual<double>>(energy, cap, warps, plan);
+    }
+    if (mixed) return plan_p3bca_t<float>(energy, cap, warps, plan);
+    return plan_p3bca_t<double>(energy, cap, warps, plan);
+}
+
+template <class S>
+static cudaError_t launch_p3bca_t(bool energy, int64_t n, const Grid &g, CellBufs &cb, double nu, double *eo,
+                                  unsigned long long *co, const P3Plan &plan, cudaStream_t st)
+{
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(cb.work_counter, 0, sizeof(unsigned int), st)) != cudaSuccess) return e;
+    if (energy)
+        k_p3bca<S, true><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, cb, nu, eo, co, cb.work_counter);
+    else
+        k_p3bca<S, false><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, cb, nu, eo, co, cb.work_counter);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_p3bca(bool mixed, bool dual, bool energy, int64_t n, const Grid &g, CellBufs &cb, double nu,
+                         double *eo, unsigned long long *co, const P3Plan &plan, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    if (dual) {
+        if (mixed) return launch_p3bca_t<Dual<float>>(energy, n, g, cb, nu, eo, co, plan, st);
+        return launch_p3bca_t<Dual<double>>(energy, n, g, cb, nu, eo, co, plan, st);
+    }
+    if (mixed) return launch_p3bca_t<float>(energy, n, g, cb, nu, eo, co, plan, st);
+    return launch_p3bca_t<double>(energy, n, g, cb, nu, eo, co, plan, st);
+}
+
+__global__ void k_unsort(int64_t n, const int32_t *__restrict__ sorted, const double *__restrict__ f0,
+                         const double *__restrict__ f1, const double *__restrict__ f2, double *o0, double *o1,
+                         double *o2)
+{
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    int32_t i = sorted[s];
+    o0[i] = f0[s];
+    o1[i] = f1[s];
+    o2[i] = f2[s];
+}
+
+cudaError_t launch_unsort(int64_t n, const CellBufs &cb, Out out, bool dual, cudaStream_t st)
+{
+    unsigned nb = (unsigned)((n + 255) / 256);
+    k_unsort<<<nb, 256, 0, st>>>(n, cb.sorted, cb.fs[0], cb.fs[1], cb.fs[2], out.fx, out.fy, out.fz);
+    if (dual) k_unsort<<<nb, 256, 0, st>>>(n, cb.sorted, cb.hs[0], cb.hs[1], cb.hs[2], out.hx, out.hy, out.hz);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Integrator (structs.hpp:40-99), FP64, in input order.  No FMA contraction, matching the
+// reference's evaluation order: x = (x + v*dt) + aX*h with h = dt*dt*0.5 (the aX quirk: the
+// acceleration vector is (aX, aX, aX)); a = g - f/m; v = v + a*(dt*0.5).
+
+__global__ void k_predictor(int64_t n, double *x, double *y, double *z, const double *vx, const double *vy,
+                            const double *vz, const double *ax, double dt)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double h = __dmul_rn(__dmul_rn(dt, dt), 0.5);
+    const double a = ax[i];
+    const double ah = __dmul_rn(a, h);
+    x[i] = __dadd_rn(__dadd_rn(x[i], __dmul_rn(vx[i], dt)), ah);
+    y[i] = __dadd_rn(__dadd_rn(y[i], __dmul_rn(vy[i], dt)), ah);
+    z[i] = __dadd_rn(__dadd_rn(z[i], __dmul_rn(vz[i], dt)), ah);
+}
+
+__global__ void k_update(int64_t n, double *vx, double *vy, double *vz, double *ax, double *ay, double *az,
+                         const double *fx, const double *fy, const double *fz, const double *m, double dt, double gx,
+                         double gy, double gz)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double h = __dmul_rn(dt, 0.5);
+    const double mi = m[i];
+    const double nx = __dsub_rn(gx, __ddiv_rn(fx[i], mi));
+    const double ny = __dsub_rn(gy, __ddiv_rn(fy[i], mi));
+    const double nz = __dsub_rn(gz, __ddiv_rn(fz[i], mi));
+    vx[i] = __dadd_rn(vx[i], __dmul_rn(nx, h));
+    vy[i] = __dadd_rn(vy[i], __dmul_rn(ny, h));
+    vz[i] = __dadd_rn(vz[i], __dmul_rn(nz, h));
+    ax[i] = nx;
+    ay[i] = ny;
+    az[i] = nz;
+}
+
+cudaError_t launch_predictor(int64_t n, double *x, double *y, double *z, const double *vx, const double *vy,
+                             const double *vz, const double *ax, double dt, cudaStream_t st)
+{
+    k_predictor<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, x, y, z, vx, vy, vz, ax, dt);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_update(int64_t n, double *vx, double *vy, double *vz, double *ax, double *ay, double *az,
+                          const double *fx, const double *fy, const double *fz, const double *m, double dt, double gx,
+                          double gy, double gz, cudaStream_t st)
+{
+    k_update<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, vx, vy, vz, ax, ay, az, fx, fy, fz, m, dt, gx, gy, gz);
+    return cudaGetLastError();
+}
+
+// per_step[*step] = *cur + constant_count; ++*step; *cur = 0   (graph-replay safe step bookkeeping)
+__global__ void k_record_count(unsigned long long *cur, unsigned long long *per_step, unsigned int *step,
+                               unsigned long long constant_count)
+{
+    unsigned int s = *step;
+    per_step[s] = *cur + constant_count;
+    *step = s + 1;
+    *cur = 0ull;
+}
+
+cudaError_t launch_record_count(unsigned long long *cur, unsigned long long *per_step, unsigned int *step,
+                                unsigned long long constant_count, cudaStream_t st)
+{
+    k_record_count<<<1, 1, 0, st>>>(cur, per_step, step, constant_count);
+    return cudaGetLastError();
+}
+
+}  // namespace tbmd

@@ -1,0 +1,352 @@
+// tbmd_main: drop-in replacement for the reference's `main` executable, running the AT three-body
+// Simulation on one GPU through the C ABI (include/tbmd.h).
+//
+// CLI (src/utility/cli.hpp:47-187): -a|--algorithm nata|auta|p3bca, -i|--iterations, -d|--delta,
+// -c|--cutoff, -gx/-gy/-gz|--gravityX/Y/Z, -csv|--csv, -o|--out, -op|--outProfile,
+// -decomp|--decomp optimal|naive, -benchyaml|--benchyaml.  Same parsing rules: a flag without a
+// value or a value that does not convert prints the help and exits 1, an unknown option is
+// reported and skipped, unset values are 0 and the algorithm defaults to NATA (the reference's
+// zero-initialised globals, main.cpp:27).  Upper-case algorithm names are accepted as well.
+// -decomp and -benchyaml only matter for MPI rank layouts and are accepted and ignored.
+// GPU options: -prec fp64|mixed, -nu V (AT strength, default 1.0 as main.cpp:41), -device N,
+// -nograph, -tune CACHE.JSONL (autotuner), -dumpfull FILE (state at %.17g after the run),
+// -parseonly (print the parsed arguments as JSON and exit without touching the GPU).
+// -op FILE writes per-step GPU timings as JSON (the reference's MEASURESIMSTEP_3BMDA line format,
+// Simulation.cpp:59-68, in nanoseconds).
+//
+// Output (Simulation.cpp:74-79, utility.cpp:54-68): with -o base.csv, after every step i the file
+// base_<i>.csv with header "ID, pX, pY, pZ, vX, vY, vZ, aX, aY, aZ, m, fX, fY, fZ", rows sorted by
+// ID, values in the default ostream format (6 significant digits).
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <iostream>
+#include <numeric>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "tbmd.h"
+
+namespace {
+
+struct Args {
+    int iterations = 0;
+    double cutoff = 0.0;
+    double deltaT = 0.0;
+    std::string inputCSV, outputCSV, outputProfile, benchYaml;
+    int algorithm = TBMD_NATA;
+    double g[3] = {0.0, 0.0, 0.0};
+    bool optimalDecomposition = false;
+    // GPU options
+    int precision = TBMD_FP64;
+    double nu = 1.0;
+    int device = 0;
+    bool graph = true;
+    bool parseOnly = false;
+    std::string tuneCache, dumpFull;
+};
+
+void printHelp()
+{
+    std::cout << "Help: \n"
+              << "Options:\n"
+              << "\t-h,--help\t\tShow this help message\n"
+              << "\t-a,--algorithm\t\talgorithm to use (\"nata\", \"p3bca\", \"auta\")\n"
+              << "\t-i,--iterations\t\tnum of iterations to simulate\n"
+              << "\t-d,--delta\t\tduration of one simulation step\n"
+              << "\t-gx,--gravityX\t\tgravitational force in x-direction\n"
+              << "\t-gy,--gravityY\t\tgravitational force in y-direction\n"
+              << "\t-gz,--gravityZ\t\tgravitational force in z-direction\n"
+              << "\t-csv,--csv\t\tcsv file with particles\n"
+              << "\t-o,--out\t\tcsv base file name that will be used to create all csv outputs from each "
+                 "simulation step\n"
+              << "-op,--outProfile\t\tjson file to save per-step timings\n"
+              << "-decomp,--decomp\t\t(optimal | naive) decomposition strategy for cart topology (ignored)\n"
+              << "-benchyaml,--benchyaml\t\tYAML file that contains config for benchmarks (ignored)\n"
+              << "\t-c,--cutoff\t\tcutoff distance\n"
+              << "GPU options:\n"
+              << "\t-prec\t\tfp64 | mixed\n\t-nu\t\tAT strength (1.0)\n\t-device\t\tCUDA device\n"
+              << "\t-nograph\t\tno CUDA graph\n\t-tune\t\tautotuner cache file\n"
+              << "\t-dumpfull\t\twrite the final state with 17 digits\n\t-parseonly\t\tprint parsed args" << std::endl;
+}
+
+[[noreturn]] void usageExit()
+{
+    printHelp();
+    std::exit(1);
+}
+
+bool isFlag(const std::string &f, const char *shortName, const char *longName)
+{
+    return f == shortName || f == longName;
+}
+
+Args parse(const std::vector<std::string> &args)
+{
+    Args a;
+    for (size_t i = 0; i < args.size(); ++i) {
+        try {
+            if (args[i].rfind("-", 0) != 0) {
+                std::cout << "CLI parser: unrecognized option: " << args[i] << std::endl;
+                continue;
+            }
+            const std::string f = args[i].substr(1);
+            auto value = [&]() -> std::string {
+                if (args.size() <= i + 1) usageExit();
+                return args[++i];
+            };
+            if (isFlag(f, "c", "-cutoff")) {
+                a.cutoff = std::stod(value());
+            } else if (isFlag(f, "i", "-iterations")) {
+                a.iterations = std::stoi(value());
+            } else if (isFlag(f, "a", "-algorithm")) {
+                std::string v = value();
+                if (v == "nata" || v == "NATA") a.algorithm = TBMD_NATA;
+                else if (v == "p3bca" || v == "P3BCA") a.algorithm = TBMD_P3BCA;
+                else if (v == "auta" || v == "AUTA") a.algorithm = TBMD_AUTA;
+                else usageExit();
+            } else if (isFlag(f, "decomp", "-decomp")) {
+                std::string v = value();
+                if (v == "optimal") a.optimalDecomposition = true;
+                else if (v == "naive") a.optimalDecomposition = false;
+                else usageExit();
+            } else if (isFlag(f, "d", "-delta")) {
+                a.deltaT = std::stod(value());
+            } else if (isFlag(f, "csv", "-csv")) {
+                a.inputCSV = value();
+            } else if (isFlag(f, "o", "-out")) {
+                a.outputCSV = value();
+            } else if (isFlag(f, "op", "-outProfile")) {
+                a.outputProfile = value();
+            } else if (isFlag(f, "benchyaml", "-benchyaml")) {
+                a.benchYaml = value();
+            } else if (isFlag(f, "gx", "-gravityX")) {
+                a.g[0] = std::stod(value());
+            } else if (isFlag(f, "gy", "-gravityY")) {
+                a.g[1] = std::stod(value());
+            } else if (isFlag(f, "gz", "-gravityZ")) {
+                a.g[2] = std::stod(value());
+            } else if (isFlag(f, "prec", "-precision")) {
+                std::string v = value();
+                if (v == "fp64") a.precision = TBMD_FP64;
+                else if (v == "mixed") a.precision = TBMD_MIXED;
+                else usageExit();
+            } else if (isFlag(f, "nu", "-nu")) {
+                a.nu = std::stod(value());
+            } else if (isFlag(f, "device", "-device")) {
+                a.device = std::stoi(value());
+            } else if (isFlag(f, "nograph", "-nograph")) {
+                a.graph = false;
+            } else if (isFlag(f, "tune", "-tune")) {
+                a.tuneCache = value();
+            } else if (isFlag(f, "dumpfull", "-dumpfull")) {
+                a.dumpFull = value();
+            } else if (isFlag(f, "parseonly", "-parseonly")) {
+                a.parseOnly = true;
+            } else if (isFlag(f, "h", "-help")) {
+                printHelp();
+                std::exit(0);
+            } else {
+                std::cout << "CLI parser: unrecognized option: " << f << std::endl;
+            }
+        } catch (std::exception &) {
+            usageExit();
+        }
+    }
+    return a;
+}
+
+struct Particles {
+    std::vector<int32_t> id;
+    std::vector<double> col[10];  // x y z vx vy vz ax ay az m
+};
+
+// utility.cpp:14-24: header row, then ID and 10 numeric columns; further columns are ignored.
+bool readCSV(const std::string &path, Particles &p, std::string &err)
+{
+    std::ifstream in(path);
+    if (!in) {
+        err = "cannot open " + path;
+        return false;
+    }
+    std::string line;
+    std::getline(in, line);  // header
+    size_t row = 0;
+    while (std::getline(in, line)) {
+        if (!line.empty() && line.back() == '\r') line.pop_back();
+        if (line.find_first_not_of(" \t") == std::string::npos) continue;
+        std::vector<std::string> cells;
+        std::stringstream ss(line);
+        std::string c;
+        while (std::getline(ss, c, ',')) cells.push_back(c);
+        if (cells.size() < 11) {
+            err = "row " + std::to_string(row) + " has fewer than 11 columns";
+            return false;
+        }
+        char *end = nullptr;
+        long idv = std::strtol(cells[0].c_str(), &end, 10);
+        if (end == cells[0].c_str()) {
+            err = "row " + std::to_string(row) + ": bad ID";
+            return false;
+        }
+        p.id.push_back((int32_t)idv);
+        for (int k = 0; k < 10; ++k) {
+            const char *b = cells[k + 1].c_str();
+            double v = std::strtod(b, &end);
+            if (end == b) {
+                err = "row " + std::to_string(row) + ": bad number '" + cells[k + 1] + "'";
+                return false;
+            }
+            p.col[k].push_back(v);
+        }
+        ++row;
+    }
+    return true;
+}
+
+std::string stepPath(const std::string &base, int step)
+{
+    return base.substr(0, base.find_last_of('.')) + "_" + std::to_string(step) + ".csv";
+}
+
+struct State {
+    std::vector<int32_t> id;
+    std::vector<double> v[13];  // x y z vx vy vz ax ay az m fx fy fz
+};
+
+bool fetch(tbmd_ctx *ctx, int64_t n, State &s)
+{
+    s.id.resize(n);
+    for (auto &c : s.v) c.resize(n);
+    return tbmd_get_particles(ctx, s.id.data(), s.v[0].data(), s.v[1].data(), s.v[2].data(), s.v[3].data(),
+                              s.v[4].data(), s.v[5].data(), s.v[6].data(), s.v[7].data(), s.v[8].data(),
+                              s.v[9].data(), s.v[10].data(), s.v[11].data(), s.v[12].data()) == TBMD_OK;
+}
+
+// utility.cpp:54-68 (writeStepToCSVWithForces), rows sorted by ID (Simulation.cpp:127-128).
+void writeStepCSV(const std::string &path, const State &s)
+{
+    std::vector<size_t> order(s.id.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return s.id[a] < s.id[b]; });
+    std::ofstream out(path);
+    out << "ID, pX, pY, pZ, vX, vY, vZ, aX, aY, aZ, m, fX, fY, fZ\n";
+    for (size_t i : order) {
+        out << s.id[i];
+        for (int k = 0; k < 13; ++k) out << ", " << s.v[k][i];
+        out << "\n";
+    }
+}
+
+void writeFull(const std::string &path, const State &s, const std::vector<uint64_t> &counts)
+{
+    FILE *f = std::fopen(path.c_str(), "w");
+    if (!f) return;
+    for (size_t i = 0; i < counts.size(); ++i)
+        std::fprintf(f, "step %zu buffer 1 triplets %llu\n", i, (unsigned long long)counts[i]);
+    for (size_t i = 0; i < s.id.size(); ++i) {
+        std::fprintf(f, "particle %d", s.id[i]);
+        for (int k = 0; k < 13; ++k) std::fprintf(f, " %.17g", s.v[k][i]);
+        std::fprintf(f, "\n");
+    }
+    std::fclose(f);
+}
+
+}  // namespace
+
+int main(int argc, char **argv)
+{
+    std::vector<std::string> args(argv + 1, argv + argc);
+    Args a = parse(args);
+    static const char *algName[3] = {"nata", "p3bca", "auta"};
+    if (a.parseOnly) {
+        std::printf("{\"algorithm\": \"%s\", \"iterations\": %d, \"delta\": %.17g, \"cutoff\": %.17g, "
+                    "\"g\": [%.17g, %.17g, %.17g], \"csv\": \"%s\", \"out\": \"%s\", \"precision\": \"%s\", "
+                    "\"nu\": %.17g, \"device\": %d, \"graph\": %s}\n",
+                    algName[a.algorithm], a.iterations, a.deltaT, a.cutoff, a.g[0], a.g[1], a.g[2],
+                    a.inputCSV.c_str(), a.outputCSV.c_str(), a.precision == TBMD_MIXED ? "mixed" : "fp64", a.nu,
+                    a.device, a.graph ? "true" : "false");
+        return 0;
+    }
+    if (!a.benchYaml.empty()) std::cout << "note: -benchyaml is ignored (no MPI benchmark harness)" << std::endl;
+
+    Particles p;
+    std::string err;
+    if (!readCSV(a.inputCSV, p, err)) {
+        std::cerr << "error reading particles: " << err << std::endl;
+        return 1;
+    }
+    const int64_t n = (int64_t)p.id.size();
+
+    tbmd_config cfg;
+    tbmd_config_init(&cfg);
+    cfg.algorithm = a.algorithm;
+    cfg.precision = a.precision;
+    cfg.cutoff = a.algorithm == TBMD_P3BCA ? a.cutoff : 0.0;
+    cfg.dt = a.deltaT;
+    for (int d = 0; d < 3; ++d) cfg.g[d] = a.g[d];
+    cfg.nu = a.nu;
+    cfg.device = a.device;
+    cfg.use_graph = a.graph ? 1 : 0;
+    tbmd_ctx *ctx = nullptr;
+    tbmd_status st = tbmd_create(&cfg, &ctx);
+    if (st != TBMD_OK) {
+        std::cerr << "error: " << tbmd_status_string(st) << std::endl;
+        return 1;
+    }
+    auto die = [&](const char *what) {
+        std::cerr << "error in " << what << ": " << tbmd_last_error(ctx) << std::endl;
+        tbmd_destroy(ctx);
+        std::exit(1);
+    };
+    if (n > 0) {
+        const double *c = nullptr;
+        (void)c;
+        if (tbmd_set_particles(ctx, n, p.id.data(), p.col[0].data(), p.col[1].data(), p.col[2].data(),
+                               p.col[3].data(), p.col[4].data(), p.col[5].data(), p.col[6].data(), p.col[7].data(),
+                               p.col[8].data(), p.col[9].data()) != TBMD_OK)
+            die("set_particles");
+    }
+    if (!a.tuneCache.empty() && n > 0 && tbmd_autotune(ctx, a.tuneCache.c_str()) != TBMD_OK) die("autotune");
+
+    std::vector<uint64_t> counts;
+    std::vector<long long> stepNs;
+    State s;
+    if (n > 0 && a.iterations > 0) {
+        const bool perStep = !a.outputCSV.empty() || !a.outputProfile.empty();
+        if (perStep) {
+            for (int i = 0; i < a.iterations; ++i) {
+                uint64_t c = 0;
+                auto t0 = std::chrono::steady_clock::now();
+                if (tbmd_step(ctx, 1, &c) != TBMD_OK) die("step");
+                auto t1 = std::chrono::steady_clock::now();
+                stepNs.push_back(std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count());
+                counts.push_back(c);
+                if (!a.outputCSV.empty()) {
+                    if (!fetch(ctx, n, s)) die("get_particles");
+                    writeStepCSV(stepPath(a.outputCSV, i), s);
+                }
+            }
+        } else {
+            counts.resize(a.iterations);
+            if (tbmd_step(ctx, a.iterations, counts.data()) != TBMD_OK) die("step");
+        }
+    }
+    if (!a.outputProfile.empty()) {
+        std::ofstream prof(a.outputProfile);
+        prof << "[";
+        for (size_t i = 0; i < stepNs.size(); ++i)
+            prof << (i ? ", " : "") << "{\"allTimes\": [" << stepNs[i] << "], \"max\": " << stepNs[i]
+                 << ", \"triplets\": " << counts[i] << "}";
+        prof << "]\n";
+    }
+    if (!a.dumpFull.empty() && n > 0) {
+        if (!fetch(ctx, n, s)) die("get_particles");
+        writeFull(a.dumpFull, s, counts);
+    }
+    tbmd_destroy(ctx);
+    return 0;
+}
