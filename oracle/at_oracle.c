@@ -220,13 +220,14 @@ void tbo_cell_dims(const double *L, double cutoff, int *dims, double *width)
     }
 }
 
+/* A non-finite coordinate lands in cell 0 (same rule as the CUDA cell build). */
 static inline int cell_coord(double x, double lo, double w, int nd)
 {
     double t = floor((x - lo) / w);
     double m = fmod(t, (double)nd);
     if (m < 0) m += (double)nd;
-    int c = (int)m;
-    return c >= nd ? nd - 1 : c;
+    if (!(m >= 0.0 && m < (double)nd)) return 0;
+    return (int)m;
 }
 
 void tbo_cell_assign(int64_t n, const double *x, const double *y, const double *z, double cutoff, const double *L,

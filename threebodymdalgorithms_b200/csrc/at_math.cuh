@@ -7,7 +7,7 @@
 //   c = |x_k - x_j|^2 = a + b - 2p,  q = u.(x_k - x_j) = p - a,  s = v.(x_k - x_j) = b - p
 //   D = p q s,  t = (a b c)^(-1/2)
 //   E = nu (1 + 3 cos g1 cos g2 cos g3) / (r1 r2 r3)^3 = nu t^3 (1 - 3 D t^2)
-// and the gradient of E(a, b, p) (c, q, s eliminated) is
+// and the gradient of E(a, b, p) (c, q, s eliminated through c = a + b - 2p, q = p - a, s = b - p) is
 //   grad_j E = alpha u + gamma v,   grad_k E = beta v + gamma u,   grad_i E = -(grad_j E + grad_k E)
 // with alpha = 2 dE/da, beta = 2 dE/db, gamma = dE/dp:
 //   m = -3 nu t^5,  B2 = m + 15 nu t^5 D t^2
@@ -67,32 +67,59 @@ struct ATCoef {
     S alpha, beta, gamma;
 };
 
-// Coefficients of one triplet.  `valid` false gives exact zeros (masked lanes, k <= j, padding)
-// without evaluating anything that could be inf or NaN in the result.  nu3 = -3 nu, nu15 = 15 nu.
-// ENERGY adds the triplet energy nu t^3 (1 - 3 D t^2) to `e`.
+// Shared core of one triplet from the six scalars a = u.u, b = v.v, c = w.w, p = u.v, q = u.w,
+// s = v.w with w = x_k - x_j.  Callers form each as a direct dot product of accurate edge vectors
+// (never c = a + b - 2p, which cancels when j and k are close but far from i).  `valid` false
+// gives exact zeros (masked lanes, k <= j, padding) without anything inf or NaN reaching the
+// result.  nu3 = -3 nu, nu15 = 15 nu.  Returns m = -3 nu t^5 and B2 = m + 15 nu t^5 D t^2; ENERGY
+// adds the triplet energy nu t^3 (1 - 3 D t^2) to `e`.
 template <bool ENERGY, class S>
-__device__ __forceinline__ ATCoef<S> at_coef(S a, S b, S p, S nu, S nu3, S nu15, bool valid, S &e)
+__device__ __forceinline__ void at_core(S a, S b, S c, S p, S q, S s, S nu, S nu3, S nu15, bool valid, S &e, S &m,
+                                        S &B2)
 {
-    S c = fma_(cst(a, -2.0), p, a + b);
-    S q = p - a;
-    S s = b - p;
-    S ab = a * b;
-    S t = rsqrt_(ab * c);
+    S t = rsqrt_(a * b * c);
     if (!valid) t = zero_like(t);
     S t2 = t * t;
     S t5 = t2 * t2 * t;
-    S pq = p * q;
-    S ps = p * s;
-    S D = pq * s;
-    S Dt2 = D * t2;
-    S m = nu3 * t5;
-    S B2 = t5 * fma_(nu15, Dt2, nu3);
+    S Dt2 = p * q * s * t2;
+    m = nu3 * t5;
+    B2 = t5 * fma_(nu15, Dt2, nu3);
+    if (ENERGY) e = e + t2 * t * fma_(nu3, Dt2, nu);
+}
+
+// Gradient coefficients for all three particles (see the top of this file).
+template <bool ENERGY, class S>
+__device__ __forceinline__ ATCoef<S> at_coef(S a, S b, S c, S p, S q, S s, S nu, S nu3, S nu15, bool valid, S &e)
+{
+    S m, B2;
+    at_core<ENERGY>(a, b, c, p, q, s, nu, nu3, nu15, valid, e, m, B2);
+    S pq = p * q, ps = p * s;
     S m2 = m + m;
     ATCoef<S> r;
     r.alpha = fma_(B2, b * (a + c), -(m2 * ps));
     r.beta = fma_(B2, a * (b + c), m2 * pq);
-    r.gamma = fma_(m, fma_(q, s, ps - pq), -(B2 * ab));
-    if (ENERGY) e = e + t2 * t * fma_(nu3, Dt2, nu);
+    r.gamma = fma_(m, fma_(q, s, ps - pq), -(B2 * (a * b)));
+    return r;
+}
+
+// Gradient on particle i alone, in the basis (u, w):  grad_i E = -(sigma u + tau w) with
+//   sigma = alpha + beta + 2 gamma = B2 c (a + b) + 2 m q s
+//   tau   = beta + gamma          = B2 a c + m (q s + p s + p q).
+// Summing alpha + gamma etc. numerically would cancel the large d/dc terms when i is far from a
+// close pair (j, k); these closed forms do not.
+template <class S>
+struct ATSelf {
+    S sigma, tau;
+};
+template <bool ENERGY, class S>
+__device__ __forceinline__ ATSelf<S> at_self(S a, S b, S c, S p, S q, S s, S nu, S nu3, S nu15, bool valid, S &e)
+{
+    S m, B2;
+    at_core<ENERGY>(a, b, c, p, q, s, nu, nu3, nu15, valid, e, m, B2);
+    S qs = q * s;
+    ATSelf<S> r;
+    r.sigma = fma_(B2, c * (a + b), (m + m) * qs);
+    r.tau = fma_(B2, a * c, m * fma_(p, q + s, qs));
     return r;
 }
 

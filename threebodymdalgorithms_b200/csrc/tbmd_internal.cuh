@@ -146,6 +146,43 @@ __device__ __forceinline__ double acc_value(double a) { return a; }
 __device__ __forceinline__ double acc_value(Dual<double> a) { return a.v; }
 
 // ---------------------------------------------------------------------------------------------
+// Edge vectors.  A displacement from vertex i is formed in FP64 and rounded once to S.  For the
+// mixed form (S = float) the rounding remainder is kept as a second float ("lo"), so that the third
+// edge w = v - u = (v_hi - u_hi) + (v_lo - u_lo) is accurate to a relative FP32 epsilon even when
+// j and k are close to each other and far from i (v_hi - u_hi is then exact by Sterbenz's lemma).
+// For double and the dual types the lo part is identically zero and compiled away.
+
+template <class S>
+struct HasLo {
+    static constexpr bool value = false;
+};
+template <>
+struct HasLo<float> {
+    static constexpr bool value = true;
+};
+
+// hi and lo parts of one FP64 displacement component (plus its tangent for dual types)
+template <class S>
+__device__ __forceinline__ void split(double d, double t, S &hi, S &lo)
+{
+    hi = make_s<S>(d, t);
+    lo = szero<S>();
+}
+template <>
+__device__ __forceinline__ void split<float>(double d, double, float &hi, float &lo)
+{
+    hi = (float)d;
+    lo = (float)(d - (double)hi);
+}
+
+template <class S>
+__device__ __forceinline__ V3<S> third_edge(V3<S> uh, V3<S> ul, V3<S> vh, V3<S> vl)
+{
+    if (HasLo<S>::value) return (vh - uh) + (vl - ul);
+    return vh - uh;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Kernel argument blocks.
 
 // Positions (FP64 SoA) and, for the adjoint, the direction vector (cotangent on the forces).

@@ -7,8 +7,9 @@
 //                shuffle per tile step) so that after 32 steps lane l holds the complete sum for
 //                k = tile + l and writes it with one FP64 atomic.  i's force is -(sum of the j- and
 //                k-side totals) by translation invariance, so it costs nothing per triplet.
-//   k_nata       NATA: all triplets seen from each particle i; only grad_i is accumulated, no
-//                atomics; per-(i, j-block) partial sums are reduced in a fixed order (deterministic).
+//   k_nata       NATA: all triplets seen from each particle i; only grad_i is accumulated (in the
+//                well-conditioned (u, w) form of at_self), no atomics; per-(i, j-block) partial
+//                sums are reduced in a fixed order (deterministic).
 //   k_cell_*     P3BCA cell grid: wrap-and-bin (FP64, same arithmetic as the oracle), counting sort
 //                by cell, stable within a cell.
 //   k_neighbors  half neighbour lists (sorted index t > s) with the reference's exact FP64
@@ -33,9 +34,24 @@
 
 namespace tbmd {
 
+// One k entry staged in shared memory: edge v from i (hi part), b = v.v, and for the mixed form
+// the lo part of v.
 template <class S>
 struct Tile {
     S vx, vy, vz, b;
+    __device__ __forceinline__ V3<S> lo() const { return vzero<S>(); }
+    __device__ __forceinline__ void set_lo(V3<S>) {}
+};
+template <>
+struct Tile<float> {
+    float vx, vy, vz, b, lx, ly, lz, pad;
+    __device__ __forceinline__ V3<float> lo() const { return {lx, ly, lz}; }
+    __device__ __forceinline__ void set_lo(V3<float> l)
+    {
+        lx = l.x;
+        ly = l.y;
+        lz = l.z;
+    }
 };
 
 template <class S>
@@ -50,15 +66,25 @@ __device__ __forceinline__ V3<A> warp_sum3(V3<A> v)
     return {warp_sum(v.x), warp_sum(v.y), warp_sum(v.z)};
 }
 
-// Displacement x_j - x_i as S: FP64 subtraction, then one rounding; the tangent carries d_j - d_i.
+// Edge x_j - x_i: FP64 subtraction, then hi/lo split (see split); the tangent carries d_j - d_i.
 template <class S>
-__device__ __forceinline__ V3<S> disp(const Pos &p, int64_t j, double xi, double yi, double zi, double dxi,
-                                      double dyi, double dzi)
+__device__ __forceinline__ void edge(const Pos &p, int64_t j, double xi, double yi, double zi, double dxi, double dyi,
+                                     double dzi, V3<S> &h, V3<S> &l)
 {
-    if (Traits<S>::dual)
-        return {make_s<S>(p.x[j] - xi, p.dx[j] - dxi), make_s<S>(p.y[j] - yi, p.dy[j] - dyi),
-                make_s<S>(p.z[j] - zi, p.dz[j] - dzi)};
-    return {make_s<S>(p.x[j] - xi, 0.0), make_s<S>(p.y[j] - yi, 0.0), make_s<S>(p.z[j] - zi, 0.0)};
+    const bool dual = Traits<S>::dual;
+    split<S>(p.x[j] - xi, dual ? p.dx[j] - dxi : 0.0, h.x, l.x);
+    split<S>(p.y[j] - yi, dual ? p.dy[j] - dyi : 0.0, h.y, l.y);
+    split<S>(p.z[j] - zi, dual ? p.dz[j] - dzi : 0.0, h.z, l.z);
+}
+
+// The six scalars of a triplet from the edges u, v (hi/lo) of vertex i; c, q and s come from the
+// third edge itself, so no scalar is a difference of nearly equal numbers.
+template <bool ENERGY, class S>
+__device__ __forceinline__ ATCoef<S> triplet(V3<S> uh, V3<S> ul, S a, V3<S> vh, V3<S> vl, S b, S nu, S nu3, S nu15,
+                                             bool valid, S &e)
+{
+    const V3<S> w = third_edge(uh, ul, vh, vl);
+    return at_coef<ENERGY>(a, b, dot3(w, w), dot3(uh, vh), dot3(uh, w), dot3(vh, w), nu, nu3, nu15, valid, e);
 }
 
 // Decode a sweep work item: block b with prefix[b] <= w < prefix[b+1], i = w - prefix[b].
@@ -105,7 +131,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
             dyi = pos.dy[i];
             dzi = pos.dz[i];
         }
-        V3<S> u[R];
+        V3<S> u[R], ul[R];
         S aa[R];
         int64_t jj[R];
         bool jv[R];
@@ -114,7 +140,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
         for (int r = 0; r < R; ++r) {
             jj[r] = (int64_t)b * JB + r * 32 + lane;
             jv[r] = jj[r] > i && jj[r] < n;
-            u[r] = jv[r] ? disp<S>(pos, jj[r], xi, yi, zi, dxi, dyi, dzi) : vzero<S>();
+            u[r] = vzero<S>();
+            ul[r] = vzero<S>();
+            if (jv[r]) edge<S>(pos, jj[r], xi, yi, zi, dxi, dyi, dzi, u[r], ul[r]);
             aa[r] = dot3(u[r], u[r]);
             fj[r] = widen(vzero<S>());
         }
@@ -122,8 +150,17 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
         for (int64_t kt = (int64_t)b * JB; kt < n; kt += 32) {
             const int64_t k = kt + lane;
             const bool kv = k < n;
-            const V3<S> vk = kv ? disp<S>(pos, k, xi, yi, zi, dxi, dyi, dzi) : vzero<S>();
-            tile[wib][lane] = {vk.x, vk.y, vk.z, dot3(vk, vk)};
+            V3<S> vk = vzero<S>(), vkl = vzero<S>();
+            if (kv) edge<S>(pos, k, xi, yi, zi, dxi, dyi, dzi, vk, vkl);
+            {
+                Tile<S> tl;
+                tl.vx = vk.x;
+                tl.vy = vk.y;
+                tl.vz = vk.z;
+                tl.b = dot3(vk, vk);
+                tl.set_lo(vkl);
+                tile[wib][lane] = tl;
+            }
             __syncwarp();
             S al[R];
             V3<S> gv[R];
@@ -140,12 +177,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
                 const int kk = (lane + t) & 31;
                 const Tile<S> e = tile[wib][kk];
                 const V3<S> v = {e.vx, e.vy, e.vz};
+                const V3<S> vl = e.lo();
                 const int64_t kidx = kt + kk;
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const bool valid = jv[r] && kidx > jj[r] && kidx < n;
-                    const S p = dot3(u[r], v);
-                    const ATCoef<S> cf = at_coef<ENERGY>(aa[r], e.b, p, nu, nu3, nu15, valid, en);
+                    const ATCoef<S> cf = triplet<ENERGY>(u[r], ul[r], aa[r], v, vl, e.b, nu, nu3, nu15, valid, en);
                     al[r] = al[r] + cf.alpha;
                     gv[r] = fma3(v, cf.gamma, gv[r]);
                     bsum = bsum + cf.beta;
@@ -207,7 +244,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_nata(int64_t n, Pos pos, double 
         const int b = (int)((int64_t)w / n);
         const int64_t i = (int64_t)w - (int64_t)b * n;
         const double xi = pos.x[i], yi = pos.y[i], zi = pos.z[i];
-        V3<S> u[R];
+        V3<S> u[R], ul[R];
         S aa[R];
         int64_t jj[R];
         bool jv[R];
@@ -215,40 +252,51 @@ __global__ void __launch_bounds__(WARPS * 32) k_nata(int64_t n, Pos pos, double 
         for (int r = 0; r < R; ++r) {
             jj[r] = (int64_t)b * JB + r * 32 + lane;
             jv[r] = jj[r] < n && jj[r] != i;
-            u[r] = jv[r] ? disp<S>(pos, jj[r], xi, yi, zi, 0.0, 0.0, 0.0) : vzero<S>();
+            u[r] = vzero<S>();
+            ul[r] = vzero<S>();
+            if (jv[r]) edge<S>(pos, jj[r], xi, yi, zi, 0.0, 0.0, 0.0, u[r], ul[r]);
             aa[r] = dot3(u[r], u[r]);
         }
         V3<Acc> g = widen(vzero<S>());
         for (int64_t kt = (int64_t)b * JB; kt < n; kt += 32) {
             const int64_t k = kt + lane;
-            const V3<S> vk = (k < n) ? disp<S>(pos, k, xi, yi, zi, 0.0, 0.0, 0.0) : vzero<S>();
-            tile[wib][lane] = {vk.x, vk.y, vk.z, dot3(vk, vk)};
+            V3<S> vk = vzero<S>(), vkl = vzero<S>();
+            if (k < n) edge<S>(pos, k, xi, yi, zi, 0.0, 0.0, 0.0, vk, vkl);
+            {
+                Tile<S> tl;
+                tl.vx = vk.x;
+                tl.vy = vk.y;
+                tl.vz = vk.z;
+                tl.b = dot3(vk, vk);
+                tl.set_lo(vkl);
+                tile[wib][lane] = tl;
+            }
             __syncwarp();
             S A[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) A[r] = szero<S>();
-            V3<S> Bv = vzero<S>();
+            V3<S> Tw = vzero<S>();
             S en = szero<S>();
 #pragma unroll 2
             for (int t = 0; t < 32; ++t) {
                 const Tile<S> e = tile[wib][t];
                 const V3<S> v = {e.vx, e.vy, e.vz};
+                const V3<S> vl = e.lo();
                 const int64_t kidx = kt + t;
                 const bool kv = kidx < n && kidx != i;
-                S bs = szero<S>();
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const bool valid = jv[r] && kv && kidx > jj[r];
-                    const S p = dot3(u[r], v);
                     S e_r = szero<S>();
-                    const ATCoef<S> cf = at_coef<ENERGY>(aa[r], e.b, p, nu, nu3, nu15, valid, e_r);
+                    const V3<S> w = third_edge(u[r], ul[r], v, vl);
+                    const ATSelf<S> cf = at_self<ENERGY>(aa[r], e.b, dot3(w, w), dot3(u[r], v), dot3(u[r], w),
+                                                         dot3(v, w), nu, nu3, nu15, valid, e_r);
                     if (ENERGY && i < jj[r]) en = en + e_r;
-                    A[r] = A[r] + (cf.alpha + cf.gamma);
-                    bs = bs + (cf.beta + cf.gamma);
+                    A[r] = A[r] + cf.sigma;
+                    Tw = fma3(w, cf.tau, Tw);
                 }
-                Bv = fma3(v, bs, Bv);
             }
-            V3<S> gt = Bv;
+            V3<S> gt = Tw;
 #pragma unroll
             for (int r = 0; r < R; ++r) gt = fma3(u[r], A[r], gt);
             g = g + widen(gt);
@@ -383,13 +431,14 @@ cudaError_t launch_nata_reduce(bool, int64_t n, int nblocks, const double *parti
 // ---------------------------------------------------------------------------------------------
 // P3BCA cell grid.  Arithmetic without FMA contraction so that it equals the oracle's C code.
 
+// A non-finite coordinate (a run that blew up) lands in cell 0, never outside the grid.
 __device__ __forceinline__ int cell_coord(double x, double lo, double w, int nd)
 {
     double t = floor(__ddiv_rn(__dsub_rn(x, lo), w));
     double m = fmod(t, (double)nd);
     if (m < 0) m = __dadd_rn(m, (double)nd);
-    int c = (int)m;
-    return c >= nd ? nd - 1 : c;
+    if (!(m >= 0.0 && m < (double)nd)) return 0;
+    return (int)m;
 }
 
 // Particle::GetSqrDistPeriodic (structs.hpp:106-115), evaluated in the reference's order.
@@ -576,8 +625,11 @@ __device__ __forceinline__ void satomic_add<Dual<float>>(Dual<float> *p, Dual<fl
 
 template <class S>
 struct SlotLayout {
-    // per-warp shared memory: [cap] of each
-    static constexpr size_t bytes_per_slot = 4 * sizeof(S) + 3 * sizeof(double) + 3 * sizeof(S) + sizeof(int32_t);
+    // per-warp shared memory, [cap] of each: FP64 position (3), edge hi + b (4 S), edge lo (3 S, mixed
+    // only), gradient accumulator (3 S), neighbour index
+    static constexpr int nlo = HasLo<S>::value ? 3 : 0;
+    static constexpr size_t bytes_per_slot =
+        3 * sizeof(double) + (4 + nlo + 3) * sizeof(S) + sizeof(int32_t);
 };
 
 template <class S, bool ENERGY>
@@ -597,7 +649,10 @@ __global__ void k_p3bca(int64_t n, Grid g, CellBufs cb, double nu_d, double *ene
     S *vy = vx + cap;
     S *vz = vy + cap;
     S *vb = vz + cap;
-    S *gx = vb + cap;
+    S *lx = vb + cap;  // lo parts (mixed only; zero-length otherwise)
+    S *ly = lx + (SlotLayout<S>::nlo ? cap : 0);
+    S *lz = ly + (SlotLayout<S>::nlo ? cap : 0);
+    S *gx = lz + (SlotLayout<S>::nlo ? cap : 0);
     S *gy = gx + cap;
     S *gz = gy + cap;
     int32_t *idx = (int32_t *)(gz + cap);
@@ -625,12 +680,19 @@ __global__ void k_p3bca(int64_t n, Grid g, CellBufs cb, double nu_d, double *ene
             px[e] = x;
             py[e] = y;
             pz[e] = z;
-            V3<S> v = {make_s<S>(x - xi, dual ? cb.dxs[t] - dxi : 0.0), make_s<S>(y - yi, dual ? cb.dys[t] - dyi : 0.0),
-                       make_s<S>(z - zi, dual ? cb.dzs[t] - dzi : 0.0)};
+            V3<S> v, l;
+            split<S>(x - xi, dual ? cb.dxs[t] - dxi : 0.0, v.x, l.x);
+            split<S>(y - yi, dual ? cb.dys[t] - dyi : 0.0, v.y, l.y);
+            split<S>(z - zi, dual ? cb.dzs[t] - dzi : 0.0, v.z, l.z);
             vx[e] = v.x;
             vy[e] = v.y;
             vz[e] = v.z;
             vb[e] = dot3(v, v);
+            if (SlotLayout<S>::nlo) {
+                lx[e] = l.x;
+                ly[e] = l.y;
+                lz[e] = l.z;
+            }
             gx[e] = szero<S>();
             gy[e] = szero<S>();
             gz[e] = szero<S>();
@@ -650,8 +712,12 @@ __global__ void k_p3bca(int64_t n, Grid g, CellBufs cb, double nu_d, double *ene
                 ++cnt;
                 const V3<S> u = {vx[a], vy[a], vz[a]};
                 const V3<S> v = {vx[bb], vy[bb], vz[bb]};
-                const S pp = dot3(u, v);
-                const ATCoef<S> cf = at_coef<ENERGY>(vb[a], vb[bb], pp, nu, nu3, nu15, true, en);
+                V3<S> ul = vzero<S>(), vl = vzero<S>();
+                if (SlotLayout<S>::nlo) {
+                    ul = {lx[a], ly[a], lz[a]};
+                    vl = {lx[bb], ly[bb], lz[bb]};
+                }
+                const ATCoef<S> cf = triplet<ENERGY>(u, ul, vb[a], v, vl, vb[bb], nu, nu3, nu15, true, en);
                 const V3<S> ga = fma3(u, cf.alpha, v * cf.gamma);
                 const V3<S> gb = fma3(v, cf.beta, u * cf.gamma);
                 satomic_add(gx + a, ga.x);
