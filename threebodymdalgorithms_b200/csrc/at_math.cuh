@@ -44,7 +44,14 @@ __device__ __forceinline__ double fma_(double a, double b, double c) { return fm
 template <class T>
 __device__ __forceinline__ Dual<T> fma_(Dual<T> a, Dual<T> b, Dual<T> c) { return a * b + c; }
 
-__device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
+// FP32: the hardware approximation (PTX rsqrt.approx.ftz.f32, relative error about 2^-23).  The
+// arguments a*b*c are products of squared distances and never denormal in this code.
+__device__ __forceinline__ float rsqrt_(float x)
+{
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 __device__ __forceinline__ double rsqrt_(double x) { return rsqrt(x); }
 template <class T>
 __device__ __forceinline__ Dual<T> rsqrt_(Dual<T> x)

@@ -144,6 +144,8 @@ __device__ __forceinline__ void atomic_out(const Out &o, int64_t idx, V3<Dual<do
 }
 __device__ __forceinline__ double acc_value(double a) { return a; }
 __device__ __forceinline__ double acc_value(Dual<double> a) { return a.v; }
+__device__ __forceinline__ double dual_tangent(double) { return 0.0; }
+__device__ __forceinline__ double dual_tangent(Dual<double> a) { return a.d; }
 
 // ---------------------------------------------------------------------------------------------
 // Edge vectors.  A displacement from vertex i is formed in FP64 and rounded once to S.  For the

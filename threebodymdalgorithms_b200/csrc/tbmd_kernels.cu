@@ -66,6 +66,26 @@ __device__ __forceinline__ V3<A> warp_sum3(V3<A> v)
     return {warp_sum(v.x), warp_sum(v.y), warp_sum(v.z)};
 }
 
+// Warp sum in the arithmetic type S (butterfly; every lane gets the total).
+__device__ __forceinline__ float shfl_xor_s(float v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+__device__ __forceinline__ double shfl_xor_s(double v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+template <class T>
+__device__ __forceinline__ Dual<T> shfl_xor_s(Dual<T> v, int m)
+{
+    return {shfl_xor_s(v.v, m), shfl_xor_s(v.d, m)};
+}
+template <class S>
+__device__ __forceinline__ V3<S> warp_sum3s(V3<S> v)
+{
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) {
+        v.x = v.x + shfl_xor_s(v.x, m);
+        v.y = v.y + shfl_xor_s(v.y, m);
+        v.z = v.z + shfl_xor_s(v.z, m);
+    }
+    return v;
+}
+
 // Edge x_j - x_i: FP64 subtraction, then hi/lo split (see split); the tangent carries d_j - d_i.
 template <class S>
 __device__ __forceinline__ void edge(const Pos &p, int64_t j, double xi, double yi, double zi, double dxi, double dyi,
@@ -553,114 +573,254 @@ cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, CellBufs &cb, b
 }
 
 // Half neighbour lists: for sorted particle s, every t > s in the 27 (fewer on one-cell axes)
-// neighbouring cells with periodic d^2 <= cutoff^2.  Lists longer than cap are truncated; the
-// largest length is recorded so the host can enlarge cap and recompute.
-__global__ void k_neighbors(int64_t n, Grid g, const double *__restrict__ xs, const double *__restrict__ ys,
-                            const double *__restrict__ zs, const int32_t *__restrict__ cell_start, int32_t *nbr,
-                            int32_t *nbr_count, int32_t *max_count, int cap)
+// neighbouring cells with periodic d^2 <= cutoff^2 (exact FP64 test).
+//
+// Block per cell c.  Particles are counting-sorted by cell id, so the candidates t > s of a
+// particle s in c are: the particles of c after s, and all particles of the neighbour cells with
+// id > c.  The block lists the neighbour cells with id >= c in increasing id order and stages
+// their particles (positions and sorted indices) in shared memory in that order; the candidate
+// list of the i-th particle of c is then the suffix starting at i + 1.  Warps take the particles of
+// c in turn and sweep their suffix 32 candidates at a time, writing survivors compacted by ballot.
+// A cell whose candidates exceed the staging capacity reads them from global memory instead.
+// Lists longer than cap are truncated; the largest length is recorded so the host can enlarge cap
+// and recompute.
+constexpr int NB_THREADS = 128;
+
+__global__ void __launch_bounds__(NB_THREADS) k_neighbors(Grid g, const double *__restrict__ xs,
+                                                          const double *__restrict__ ys,
+                                                          const double *__restrict__ zs,
+                                                          const int32_t *__restrict__ cell_start, int32_t *nbr,
+                                                          int32_t *nbr_count, int32_t *max_count, int cap,
+                                                          int max_stage)
 {
-    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    const double xa = xs[s], ya = ys[s], za = zs[s];
-    const int cx = cell_coord(xa, g.lo[0], g.w[0], g.dims[0]);
-    const int cy = cell_coord(ya, g.lo[1], g.w[1], g.dims[1]);
-    const int cz = cell_coord(za, g.lo[2], g.w[2], g.dims[2]);
-    int cnt = 0;
-    int32_t *dst = nbr + s * (int64_t)cap;
-    const int lz = g.dims[2] == 1 ? 0 : -1, hz = g.dims[2] == 1 ? 0 : 1;
-    const int ly = g.dims[1] == 1 ? 0 : -1, hy = g.dims[1] == 1 ? 0 : 1;
-    const int lx = g.dims[0] == 1 ? 0 : -1, hx = g.dims[0] == 1 ? 0 : 1;
-    for (int oz = lz; oz <= hz; ++oz) {
-        const int nz = (cz + oz + g.dims[2]) % g.dims[2];
-        for (int oy = ly; oy <= hy; ++oy) {
-            const int ny = (cy + oy + g.dims[1]) % g.dims[1];
-            for (int ox = lx; ox <= hx; ++ox) {
-                const int nx = (cx + ox + g.dims[0]) % g.dims[0];
-                const int nc = (nz * g.dims[1] + ny) * g.dims[0] + nx;
-                const int32_t e = cell_start[nc + 1];
-                for (int32_t t = max(cell_start[nc], (int32_t)s + 1); t < e; ++t) {
-                    if (sqdist_periodic(xa, ya, za, xs[t], ys[t], zs[t], g) > g.sqcut) continue;
-                    if (cnt < cap) dst[cnt] = t;
-                    ++cnt;
-                }
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double *sx = (double *)smraw;
+    double *sy = sx + max_stage;
+    double *sz = sy + max_stage;
+    int32_t *st = (int32_t *)(sz + max_stage);
+    __shared__ int cstart[27], cpre[28];
+    __shared__ int nk;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int NW = NB_THREADS / 32;
+    for (int64_t c = blockIdx.x; c < g.ncells; c += gridDim.x) {
+        const int b0 = cell_start[c], e0 = cell_start[c + 1];
+        if (b0 == e0) continue;
+        if (threadIdx.x == 0) {
+            const int cx = (int)(c % g.dims[0]), cy = (int)((c / g.dims[0]) % g.dims[1]),
+                      cz = (int)(c / ((int64_t)g.dims[0] * g.dims[1]));
+            int ids[27], K = 0;
+            for (int oz = (g.dims[2] == 1 ? 0 : -1); oz <= (g.dims[2] == 1 ? 0 : 1); ++oz)
+                for (int oy = (g.dims[1] == 1 ? 0 : -1); oy <= (g.dims[1] == 1 ? 0 : 1); ++oy)
+                    for (int ox = (g.dims[0] == 1 ? 0 : -1); ox <= (g.dims[0] == 1 ? 0 : 1); ++ox) {
+                        const int nx = (cx + ox + g.dims[0]) % g.dims[0];
+                        const int ny = (cy + oy + g.dims[1]) % g.dims[1];
+                        const int nz = (cz + oz + g.dims[2]) % g.dims[2];
+                        const int nc = (nz * g.dims[1] + ny) * g.dims[0] + nx;
+                        if (nc < c) continue;
+                        int q = K++;  // insertion by id (ids are distinct)
+                        while (q > 0 && ids[q - 1] > nc) {
+                            ids[q] = ids[q - 1];
+                            --q;
+                        }
+                        ids[q] = nc;
+                    }
+            int run = 0;
+            for (int k = 0; k < K; ++k) {
+                cstart[k] = cell_start[ids[k]];
+                cpre[k] = run;
+                run += cell_start[ids[k] + 1] - cstart[k];
+            }
+            cpre[K] = run;
+            nk = K;
+        }
+        __syncthreads();
+        const int K = nk, T = cpre[K];
+        const bool staged = T <= max_stage;
+        if (staged) {
+            for (int q = threadIdx.x; q < T; q += NB_THREADS) {
+                int k = 0;
+                while (k + 1 < K && cpre[k + 1] <= q) ++k;
+                const int t = cstart[k] + (q - cpre[k]);
+                sx[q] = xs[t];
+                sy[q] = ys[t];
+                sz[q] = zs[t];
+                st[q] = t;
             }
         }
+        __syncthreads();
+        for (int sl = warp; sl < e0 - b0; sl += NW) {
+            const int s = b0 + sl;  // cell c comes first in the candidate order: q = sl
+            const double xa = xs[s], ya = ys[s], za = zs[s];
+            int cnt = 0;
+            int32_t *dst = nbr + (int64_t)s * cap;
+            for (int q0 = sl + 1; q0 < T; q0 += 32) {
+                const int q = q0 + lane;
+                bool pass = false;
+                int t = 0;
+                if (q < T) {
+                    double x, y, z;
+                    if (staged) {
+                        t = st[q];
+                        x = sx[q];
+                        y = sy[q];
+                        z = sz[q];
+                    } else {
+                        int k = 0;
+                        while (k + 1 < K && cpre[k + 1] <= q) ++k;
+                        t = cstart[k] + (q - cpre[k]);
+                        x = xs[t];
+                        y = ys[t];
+                        z = zs[t];
+                    }
+                    pass = sqdist_periodic(xa, ya, za, x, y, z, g) <= g.sqcut;
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, pass);
+                const int off = cnt + __popc(m & ((1u << lane) - 1u));
+                if (pass && off < cap) dst[off] = t;
+                cnt += __popc(m);
+            }
+            if (lane == 0) {
+                nbr_count[s] = cnt;
+                atomicMax(max_count, cnt);
+            }
+        }
+        __syncthreads();
     }
-    nbr_count[s] = cnt;
-    atomicMax(max_count, cnt);
+}
+
+// Staging capacity: 2.5 times the expected candidate count (14 of the 27 cells have id >= c on
+// average), at least 256, at most 4096 (112 KiB).
+static int neighbor_stage_cap(const Grid &g, int64_t n)
+{
+    const double mean = (double)n / (double)g.ncells;
+    const int cells = (g.dims[0] == 1 ? 1 : 3) * (g.dims[1] == 1 ? 1 : 3) * (g.dims[2] == 1 ? 1 : 3);
+    int want = (int)(2.5 * mean * (cells / 2 + 1)) + 128;
+    want = (want + 31) / 32 * 32;
+    return want < 256 ? 256 : (want > 4096 ? 4096 : want);
 }
 
 cudaError_t launch_neighbors(int64_t n, const Grid &g, CellBufs &cb, cudaStream_t st)
 {
-    k_neighbors<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, g, cb.xs, cb.ys, cb.zs, cb.cell_start, cb.nbr,
-                                                            cb.nbr_count, cb.max_count, cb.cap);
+    const int max_stage = neighbor_stage_cap(g, n);
+    const size_t smem = (size_t)max_stage * (3 * sizeof(double) + sizeof(int32_t));
+    int64_t blocks = g.ncells < 65535 * 16 ? g.ncells : 65535 * 16;
+    k_neighbors<<<(unsigned)blocks, NB_THREADS, smem, st>>>(g, cb.xs, cb.ys, cb.zs, cb.cell_start, cb.nbr,
+                                                            cb.nbr_count, cb.max_count, cb.cap, max_stage);
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------------------------
-// P3BCA triplets.  Warp per sorted particle s (dynamic item counter).  The half list (a slot per
-// neighbour) is staged in the warp's shared memory: displacement from s as S and its square,
-// the FP64 position for the exact third-edge test, and an S accumulator per slot.  Lanes walk the
-// flattened list of slot pairs (a < b); each inside triplet adds its j- and k-side gradient into
-// the slot accumulators (shared atomics) and its i-side into a register.  At the end every slot
-// is flushed with one FP64 atomic.
+// P3BCA triplets.  Warp per sorted particle s (dynamic item counter).  Its half list (M slots) is
+// staged in the warp's shared memory: edge from s (hi, its square, and the lo part for the mixed
+// form), an S gradient accumulator per slot, the neighbour index and (FP64 forms) the neighbour's
+// FP64 position for the exact third-edge test.
+//
+// Every unordered slot pair is visited once, block by block (blocks of 32 slots).  For own block A
+// lane x owns slot A+x: its edge and its gradient accumulator live in registers.
+//   - pairs inside A: circular diagonals, pair (x, (x + d) mod m_A), d = 1 .. m_A/2 (on the half
+//     diagonal of an even m_A only x < m_A/2);
+//   - pairs A x B with a later block B: if B is nearly full, a rotation, pair (x, (x + t) & 31),
+//     t = 0..31; otherwise each slot of B in turn against all lanes.
+// In every warp step the partner slots are distinct, so partner gradients are added to their slot
+// with a plain shared-memory read-modify-write (one __syncwarp per step, no atomics); in the
+// broadcast steps the partner gradient is first summed over the warp.  The i-side gradient stays
+// in registers.  At the end each slot is flushed with one FP64 atomic.
+//
+// Cutoff test of the third edge.  FP64 forms: the reference's exact FP64 test (structs.hpp:106-115)
+// on the staged positions.  Mixed form: the same periodic formula in FP32 on the accurate third
+// edge (or, when no list entry of s wraps around the box and the box is at least 4 cutoffs wide,
+// the raw squared distance, which the formula then equals), decided directly outside a guard band
+// around cutoff^2 that bounds the FP32 error, and by the exact FP64 test inside it.  Counts are
+// therefore exact in both forms.
 
 template <class S>
-__device__ __forceinline__ void satomic_add(S *p, S v)
-{
-    atomicAdd(p, v);
-}
-template <>
-__device__ __forceinline__ void satomic_add<Dual<double>>(Dual<double> *p, Dual<double> v)
-{
-    atomicAdd(&p->v, v.v);
-    atomicAdd(&p->d, v.d);
-}
-template <>
-__device__ __forceinline__ void satomic_add<Dual<float>>(Dual<float> *p, Dual<float> v)
-{
-    atomicAdd(&p->v, v.v);
-    atomicAdd(&p->d, v.d);
-}
+struct alignas(4 * sizeof(S)) Slot4 {
+    S x, y, z, w;
+};
 
 template <class S>
 struct SlotLayout {
-    // per-warp shared memory, [cap] of each: FP64 position (3), edge hi + b (4 S), edge lo (3 S, mixed
-    // only), gradient accumulator (3 S), neighbour index
-    static constexpr int nlo = HasLo<S>::value ? 3 : 0;
+    // per-warp shared memory, [cap] of each: edge hi + b (Slot4), edge lo (Slot4, mixed only),
+    // gradient accumulator (3 S), neighbour index, FP64 position (3 doubles, FP64 forms only)
+    static constexpr bool mixed = HasLo<S>::value;
+    static constexpr int nlo = mixed ? 1 : 0;
+    static constexpr int npos = mixed ? 0 : 3;
     static constexpr size_t bytes_per_slot =
-        3 * sizeof(double) + (4 + nlo + 3) * sizeof(S) + sizeof(int32_t);
+        (1 + nlo) * sizeof(Slot4<S>) + npos * sizeof(double) + 3 * sizeof(S) + sizeof(int32_t);
 };
+
+template <class S>
+__device__ __forceinline__ float to_float(S v);
+template <>
+__device__ __forceinline__ float to_float<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ float to_float<double>(double v) { return (float)v; }
+template <>
+__device__ __forceinline__ float to_float<Dual<double>>(Dual<double> v) { return (float)v.v; }
+template <>
+__device__ __forceinline__ float to_float<Dual<float>>(Dual<float> v) { return v.v; }
+
+template <class S>
+struct P3Warp {
+    Slot4<S> *sd;  // hi edge + b
+    Slot4<S> *sl;  // lo edge (mixed)
+    double *px, *py, *pz;
+    S *gx, *gy, *gz;
+    int32_t *idx;
+};
+
+// Third-edge cutoff decision for slots a (own) and b (partner) with third edge w.
+template <class S>
+__device__ __forceinline__ bool cut_inside(const P3Warp<S> &W, const CellBufs &cb, const Grid &g, int a, int b,
+                                           V3<S> w, S cww, bool rawok, float band, float Lx, float Ly, float Lz)
+{
+    if (SlotLayout<S>::mixed) {
+        float d2;
+        if (rawok) {
+            d2 = to_float(cww);
+        } else {
+            const float ax = fabsf(to_float(w.x)), ay = fabsf(to_float(w.y)), az = fabsf(to_float(w.z));
+            const float mx = fminf(ax, Lx - ax), my = fminf(ay, Ly - ay), mz = fminf(az, Lz - az);
+            d2 = fmaf(mx, mx, fmaf(my, my, mz * mz));
+        }
+        const float sq = (float)g.sqcut;
+        if (d2 <= sq - band) return true;
+        if (d2 > sq + band) return false;
+        const int32_t ta = W.idx[a], tb = W.idx[b];
+        return sqdist_periodic(cb.xs[ta], cb.ys[ta], cb.zs[ta], cb.xs[tb], cb.ys[tb], cb.zs[tb], g) <= g.sqcut;
+    }
+    return sqdist_periodic(W.px[a], W.py[a], W.pz[a], W.px[b], W.py[b], W.pz[b], g) <= g.sqcut;
+}
 
 template <class S, bool ENERGY>
 __global__ void k_p3bca(int64_t n, Grid g, CellBufs cb, double nu_d, double *energy_out,
-                        unsigned long long *count_out, unsigned int *counter)
+                        unsigned long long *count_out, unsigned int *counter, float band, int raw_ok)
 {
     using Acc = typename Traits<S>::Acc;
+    using L = SlotLayout<S>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int cap = cb.cap;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    unsigned char *base = smem + (size_t)wib * cap * SlotLayout<S>::bytes_per_slot;
-    double *px = (double *)base;
-    double *py = px + cap;
-    double *pz = py + cap;
-    S *vx = (S *)(pz + cap);
-    S *vy = vx + cap;
-    S *vz = vy + cap;
-    S *vb = vz + cap;
-    S *lx = vb + cap;  // lo parts (mixed only; zero-length otherwise)
-    S *ly = lx + (SlotLayout<S>::nlo ? cap : 0);
-    S *lz = ly + (SlotLayout<S>::nlo ? cap : 0);
-    S *gx = lz + (SlotLayout<S>::nlo ? cap : 0);
-    S *gy = gx + cap;
-    S *gz = gy + cap;
-    int32_t *idx = (int32_t *)(gz + cap);
+    unsigned char *base = smem + (size_t)wib * cap * L::bytes_per_slot;
+    P3Warp<S> W;
+    W.sd = (Slot4<S> *)base;
+    W.sl = W.sd + cap;
+    double *pbase = (double *)(W.sl + (L::nlo ? cap : 0));
+    W.px = pbase;
+    W.py = pbase + (L::npos ? cap : 0);
+    W.pz = W.py + (L::npos ? cap : 0);
+    W.gx = (S *)(W.pz + (L::npos ? cap : 0));
+    W.gy = W.gx + cap;
+    W.gz = W.gy + cap;
+    W.idx = (int32_t *)(W.gz + cap);
 
     const S nu = constant<S>(nu_d), nu3 = constant<S>(-3.0 * nu_d), nu15 = constant<S>(15.0 * nu_d);
     const Out outs = {cb.fs[0], cb.fs[1], cb.fs[2], cb.hs[0], cb.hs[1], cb.hs[2]};
     const bool dual = Traits<S>::dual;
-    unsigned long long cnt = 0;
+    const float Lx = (float)g.L[0], Ly = (float)g.L[1], Lz = (float)g.L[2];
+    const double cwrap = sqrt(g.sqcut) * 1.0000001;
+    unsigned int cnt = 0;
     Acc en_acc = to_acc(szero<S>());
 
     unsigned int w = 0;
@@ -669,85 +829,165 @@ __global__ void k_p3bca(int64_t n, Grid g, CellBufs cb, double nu_d, double *ene
     while ((int64_t)w < n) {
         unsigned int wn = 0;
         if (lane == 0) wn = atomicAdd(counter, 1u);
-        const int64_t s = w;
+        const int s = (int)w;
         const int M = min(cb.nbr_count[s], cap);
         const double xi = cb.xs[s], yi = cb.ys[s], zi = cb.zs[s];
         const double dxi = dual ? cb.dxs[s] : 0.0, dyi = dual ? cb.dys[s] : 0.0, dzi = dual ? cb.dzs[s] : 0.0;
+        bool nowrap = true;
         for (int e = lane; e < M; e += 32) {
-            const int32_t t = cb.nbr[s * (int64_t)cap + e];
-            idx[e] = t;
+            const int32_t t = cb.nbr[(int64_t)s * cap + e];
+            W.idx[e] = t;
             const double x = cb.xs[t], y = cb.ys[t], z = cb.zs[t];
-            px[e] = x;
-            py[e] = y;
-            pz[e] = z;
-            V3<S> v, l;
-            split<S>(x - xi, dual ? cb.dxs[t] - dxi : 0.0, v.x, l.x);
-            split<S>(y - yi, dual ? cb.dys[t] - dyi : 0.0, v.y, l.y);
-            split<S>(z - zi, dual ? cb.dzs[t] - dzi : 0.0, v.z, l.z);
-            vx[e] = v.x;
-            vy[e] = v.y;
-            vz[e] = v.z;
-            vb[e] = dot3(v, v);
-            if (SlotLayout<S>::nlo) {
-                lx[e] = l.x;
-                ly[e] = l.y;
-                lz[e] = l.z;
+            if (L::npos) {
+                W.px[e] = x;
+                W.py[e] = y;
+                W.pz[e] = z;
             }
-            gx[e] = szero<S>();
-            gy[e] = szero<S>();
-            gz[e] = szero<S>();
+            const double ddx = x - xi, ddy = y - yi, ddz = z - zi;
+            nowrap = nowrap && fabs(ddx) <= cwrap && fabs(ddy) <= cwrap && fabs(ddz) <= cwrap;
+            V3<S> v, l;
+            split<S>(ddx, dual ? cb.dxs[t] - dxi : 0.0, v.x, l.x);
+            split<S>(ddy, dual ? cb.dys[t] - dyi : 0.0, v.y, l.y);
+            split<S>(ddz, dual ? cb.dzs[t] - dzi : 0.0, v.z, l.z);
+            W.sd[e] = Slot4<S>{v.x, v.y, v.z, dot3(v, v)};
+            if (L::nlo) W.sl[e] = Slot4<S>{l.x, l.y, l.z, szero<S>()};
+            W.gx[e] = szero<S>();
+            W.gy[e] = szero<S>();
+            W.gz[e] = szero<S>();
         }
+        const bool rawok = raw_ok && __all_sync(0xffffffffu, nowrap);
         __syncwarp();
-        const int64_t P = (int64_t)M * (M - 1) / 2;
-        // pair index p = bb*(bb-1)/2 + a with a < bb
-        int64_t p = lane;
-        int bb = (int)((1.0 + sqrt(1.0 + 8.0 * (double)p)) * 0.5);
-        while ((int64_t)bb * (bb - 1) / 2 > p) --bb;
-        while ((int64_t)(bb + 1) * bb / 2 <= p) ++bb;
-        int a = (int)(p - (int64_t)bb * (bb - 1) / 2);
-        V3<S> gi = vzero<S>();
         S en = szero<S>();
-        for (; p < P; p += 32) {
-            if (sqdist_periodic(px[a], py[a], pz[a], px[bb], py[bb], pz[bb], g) <= g.sqcut) {
-                ++cnt;
-                const V3<S> u = {vx[a], vy[a], vz[a]};
-                const V3<S> v = {vx[bb], vy[bb], vz[bb]};
-                V3<S> ul = vzero<S>(), vl = vzero<S>();
-                if (SlotLayout<S>::nlo) {
-                    ul = {lx[a], ly[a], lz[a]};
-                    vl = {lx[bb], ly[bb], lz[bb]};
+
+        for (int A0 = 0; A0 < M; A0 += 32) {
+            const int mA = min(32, M - A0);
+            const bool own = lane < mA;
+            const int a = A0 + (own ? lane : 0);
+            const Slot4<S> od = W.sd[a];
+            const V3<S> u = {od.x, od.y, od.z};
+            V3<S> ul = vzero<S>();
+            if (L::nlo) {
+                const Slot4<S> ol = W.sl[a];
+                ul = {ol.x, ol.y, ol.z};
+            }
+            const S aa = od.w;
+            V3<S> acc = vzero<S>();
+
+            // evaluate own slot a against partner slot b; returns the partner's gradient
+            auto pair = [&](bool act, int b) -> V3<S> {
+                const Slot4<S> pd = W.sd[b];
+                const V3<S> v = {pd.x, pd.y, pd.z};
+                V3<S> vl = vzero<S>();
+                if (L::nlo) {
+                    const Slot4<S> pl = W.sl[b];
+                    vl = {pl.x, pl.y, pl.z};
                 }
-                const ATCoef<S> cf = triplet<ENERGY>(u, ul, vb[a], v, vl, vb[bb], nu, nu3, nu15, true, en);
+                const V3<S> wv = third_edge(u, ul, v, vl);
+                const S cww = dot3(wv, wv);
+                bool inside = false;
+                if (act) inside = cut_inside(W, cb, g, a, b, wv, cww, rawok, band, Lx, Ly, Lz);
+                cnt += inside ? 1u : 0u;
+                const ATCoef<S> cf =
+                    at_coef<ENERGY>(aa, pd.w, cww, dot3(u, v), dot3(u, wv), dot3(v, wv), nu, nu3, nu15, inside, en);
                 const V3<S> ga = fma3(u, cf.alpha, v * cf.gamma);
                 const V3<S> gb = fma3(v, cf.beta, u * cf.gamma);
-                satomic_add(gx + a, ga.x);
-                satomic_add(gy + a, ga.y);
-                satomic_add(gz + a, ga.z);
-                satomic_add(gx + bb, gb.x);
-                satomic_add(gy + bb, gb.y);
-                satomic_add(gz + bb, gb.z);
-                gi = gi + ga + gb;
+                acc = acc + ga;
+                return gb;
+            };
+
+            // pairs inside block A: circular diagonals
+            for (int d = 1; 2 * d <= mA; ++d) {
+                int y = lane + d;
+                if (y >= mA) y -= mA;
+                const bool act = own && (2 * d < mA || lane < d);
+                const int b = A0 + (y < mA ? y : 0);  // lanes past the block read a valid slot, masked
+                const V3<S> gb = pair(act, b);
+                if (act) {
+                    W.gx[b] = W.gx[b] + gb.x;
+                    W.gy[b] = W.gy[b] + gb.y;
+                    W.gz[b] = W.gz[b] + gb.z;
+                }
+                __syncwarp();
             }
-            a += 32;
-            while (a >= bb) {
-                a -= bb;
-                ++bb;
+            // pairs A x B with every later block
+            for (int B0 = A0 + 32; B0 < M; B0 += 32) {
+                const int mB = min(32, M - B0);
+                if (mB >= 24) {
+                    for (int t = 0; t < 32; ++t) {
+                        const int y = (lane + t) & 31;
+                        const bool act = own && y < mB;
+                        const int b = B0 + (y < mB ? y : 0);
+                        const V3<S> gb = pair(act, b);
+                        if (act) {
+                            W.gx[b] = W.gx[b] + gb.x;
+                            W.gy[b] = W.gy[b] + gb.y;
+                            W.gz[b] = W.gz[b] + gb.z;
+                        }
+                        __syncwarp();
+                    }
+                } else {
+                    for (int y = 0; y < mB; ++y) {
+                        const int b = B0 + y;
+                        const V3<S> gb = warp_sum3s(pair(own, b));
+                        if (lane == 0) {
+                            W.gx[b] = W.gx[b] + gb.x;
+                            W.gy[b] = W.gy[b] + gb.y;
+                            W.gz[b] = W.gz[b] + gb.z;
+                        }
+                        __syncwarp();
+                    }
+                }
             }
+            // merge the own accumulator into its slot
+            if (own) {
+                W.gx[a] = W.gx[a] + acc.x;
+                W.gy[a] = W.gy[a] + acc.y;
+                W.gz[a] = W.gz[a] + acc.z;
+            }
+            __syncwarp();
         }
-        __syncwarp();
-        for (int e = lane; e < M; e += 32) atomic_out(outs, idx[e], widen(V3<S>{gx[e], gy[e], gz[e]}));
-        V3<Acc> gia = warp_sum3(widen(gi));
+
+        // flush the slots; i's gradient is minus the sum of all slot gradients (translation invariance)
+        V3<Acc> gia = widen(vzero<S>());
+        for (int e = lane; e < M; e += 32) {
+            const V3<Acc> ge = widen(V3<S>{W.gx[e], W.gy[e], W.gz[e]});
+            atomic_out(outs, W.idx[e], ge);
+            gia = gia + ge;
+        }
+        gia = warp_sum3(gia);
         if (lane == 0) atomic_out(outs, s, V3<Acc>{-gia.x, -gia.y, -gia.z});
         if (ENERGY) en_acc = en_acc + to_acc(en);
         __syncwarp();
         w = __shfl_sync(0xffffffffu, wn, 0);
     }
-    cnt = warp_sum_u64(cnt);
-    if (lane == 0 && count_out) atomicAdd(count_out, cnt);
+    unsigned long long c64 = warp_sum_u64((unsigned long long)cnt);
+    if (lane == 0 && count_out) atomicAdd(count_out, c64);
     if (ENERGY) {
         en_acc = warp_sum(en_acc);
         if (lane == 0) atomicAdd(energy_out, acc_value(en_acc));
     }
+}
+
+// Half-width of the FP32 uncertainty band around cutoff^2 of the mixed test.  Each FP32 component
+// of the third edge (two-float difference of edges from i, then L - |d|) is within
+// e = 16 eps32 (max L + cutoff) of the FP64 value; the squared periodic distance is then within
+// 2 sqrt(3) c e + 3 e^2 plus its own FP32 rounding (8 eps32 c^2).  Four times that is used.
+static float guard_band(const Grid &g)
+{
+    const double eps = 1.0 / 8388608.0;  // 2^-23
+    const double c = sqrt(g.sqcut);
+    const double Lm = fmax(g.L[0], fmax(g.L[1], g.L[2]));
+    const double e = 16.0 * eps * (Lm + c);
+    return (float)(4.0 * (2.0 * 1.7320508075688772 * c * e + 3.0 * e * e + 8.0 * eps * g.sqcut));
+}
+
+// The raw squared distance equals the periodic formula for two neighbours of s that do not wrap
+// (each within the cutoff of s per axis, so within 2 cutoffs of each other) when every box length
+// is at least 4 cutoffs: then min(|d|, L - |d|) = |d| exactly.
+static int raw_test_ok(const Grid &g)
+{
+    const double c = sqrt(g.sqcut) * 1.0000001;
+    return (g.L[0] >= 4.0 * c && g.L[1] >= 4.0 * c && g.L[2] >= 4.0 * c) ? 1 : 0;
 }
 
 template <class S>
@@ -777,6 +1017,10 @@ static cudaError_t plan_p3bca_t(bool energy, int cap, int warps, P3Plan *plan)
 
 cudaError_t plan_p3bca(bool mixed, bool dual, bool energy, int cap, int warps, P3Plan *plan)
 {
+    // the neighbour kernel's largest staging size (4096 candidates), set once outside any capture
+    cudaError_t e0 = cudaFuncSetAttribute(k_neighbors, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)(4096 * (3 * sizeof(double) + sizeof(int32_t))));
+    if (e0 != cudaSuccess) return e0;
     if (dual) {
         if (mixed) return plan_p3bca_t<Dual<float>>(energy, cap, warps, plan);
         return plan_p3bca_t<Dual<double>>(energy, cap, warps, plan);
@@ -792,9 +1036,11 @@ static cudaError_t launch_p3bca_t(bool energy, int64_t n, const Grid &g, CellBuf
     cudaError_t e;
     if ((e = cudaMemsetAsync(cb.work_counter, 0, sizeof(unsigned int), st)) != cudaSuccess) return e;
     if (energy)
-        k_p3bca<S, true><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, cb, nu, eo, co, cb.work_counter);
+        k_p3bca<S, true><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, cb, nu, eo, co, cb.work_counter,
+                                                                         guard_band(g), raw_test_ok(g));
     else
-        k_p3bca<S, false><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, cb, nu, eo, co, cb.work_counter);
+        k_p3bca<S, false><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, cb, nu, eo, co, cb.work_counter,
+                                                                          guard_band(g), raw_test_ok(g));
     return cudaGetLastError();
 }
 
