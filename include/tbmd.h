@@ -40,7 +40,8 @@ typedef enum {
     TBMD_CAPACITY_RETRY = 4,  /* neighbour capacity still too small after the automatic retries */
     TBMD_CUDA_ERROR = 5,      /* a CUDA runtime call failed; see tbmd_last_error */
     TBMD_TIMEOUT = 6,         /* a bounded device-side wait gave up (the kernel returned early) */
-    TBMD_NO_DEVICE = 7        /* no CUDA device, or not an sm_100 device */
+    TBMD_NO_DEVICE = 7,       /* no CUDA device, or not an sm_100 device */
+    TBMD_TOO_LARGE = 8        /* n above the limit of an allocation-free entry point */
 } tbmd_status;
 
 /* Same numbering as the reference's AlgorithmType (src/utility/enums.hpp). */
@@ -157,6 +158,21 @@ const char *tbmd_tuning(const tbmd_ctx *ctx);
  * executions) and launches (kernels launched in the phase) and returns the number of phases. */
 tbmd_status tbmd_set_profiling(tbmd_ctx *ctx, int32_t on);
 int32_t tbmd_phase_times(const tbmd_ctx *ctx, double *ms, uint64_t *calls, uint64_t *launches, int32_t max);
+
+/* Allocation-free NATA forces.  No counterpart in the reference: this entry point exists for
+ * callers that cannot allocate device memory when they need forces (a fixed pre-reserved memory
+ * budget, a callback inside another library that owns the allocator, a latency-critical loop that
+ * must not synchronise in cudaMalloc).  It needs no context: positions x, y, z and forces fx, fy, fz
+ * are caller device buffers of n doubles, and the only scratch is a fixed static device array of
+ * about 3 MiB inside the library (held on every GPU that loads it until exit).  It computes the
+ * stored forces (+grad E, no cutoff, strength nu) of all C(n,3) triplets with the NATA kernel in
+ * FP64 or mixed precision on `stream` (cudaStream_t, NULL = legacy default stream), asynchronously.
+ * 1 <= n <= TBMD_NOALLOC_MAX_N; larger n returns TBMD_TOO_LARGE without launching anything.  The
+ * first call on a device looks up the scratch address (make it before any stream capture).  All
+ * calls share the scratch, so calls that overlap on the GPU race and must be serialised. */
+#define TBMD_NOALLOC_MAX_N 4096
+tbmd_status tbmd_nata_forces_noalloc(int64_t n, const double *x, const double *y, const double *z, double nu,
+                                     int32_t precision, double *fx, double *fy, double *fz, void *stream);
 
 /* Wait for all work of the context's stream. */
 tbmd_status tbmd_sync(tbmd_ctx *ctx);

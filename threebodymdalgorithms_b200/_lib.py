@@ -15,14 +15,15 @@ ALGORITHMS = {"nata": NATA, "p3bca": P3BCA, "auta": AUTA}
 PRECISIONS = {"fp64": FP64, "mixed": MIXED}
 
 STATUS = {0: "TBMD_OK", 1: "TBMD_INVALID_ARG", 2: "TBMD_BAD_INPUT", 3: "TBMD_NOT_READY", 4: "TBMD_CAPACITY_RETRY",
-          5: "TBMD_CUDA_ERROR", 6: "TBMD_TIMEOUT", 7: "TBMD_NO_DEVICE"}
+          5: "TBMD_CUDA_ERROR", 6: "TBMD_TIMEOUT", 7: "TBMD_NO_DEVICE", 8: "TBMD_TOO_LARGE"}
+NOALLOC_MAX_N = 4096
 
 # every symbol declared in include/tbmd.h
 EXPORTS = ("tbmd_config_init", "tbmd_create", "tbmd_destroy", "tbmd_last_error", "tbmd_status_string",
            "tbmd_abi_version", "tbmd_set_particles", "tbmd_get_particles", "tbmd_num_particles", "tbmd_step",
            "tbmd_forces", "tbmd_adjoint", "tbmd_forces_device", "tbmd_adjoint_device", "tbmd_set_domain",
            "tbmd_cells", "tbmd_batch_forces", "tbmd_batch_adjoint", "tbmd_autotune", "tbmd_tuning", "tbmd_sync",
-           "tbmd_kernel_launches", "tbmd_set_profiling", "tbmd_phase_times")
+           "tbmd_kernel_launches", "tbmd_set_profiling", "tbmd_phase_times", "tbmd_nata_forces_noalloc")
 PHASES = ("predictor", "cells", "neighbors", "triplets", "update")
 
 
@@ -76,6 +77,7 @@ def load():
         "tbmd_kernel_launches": (C.c_uint64, [vp]),
         "tbmd_set_profiling": (C.c_int, [vp, i32]),
         "tbmd_phase_times": (i32, [vp, d, pu64, pu64, i32]),
+        "tbmd_nata_forces_noalloc": (C.c_int, [i64, vp, vp, vp, C.c_double, i32, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -462,6 +462,7 @@ const char *tbmd_status_string(tbmd_status s)
         case TBMD_CUDA_ERROR: return "CUDA error";
         case TBMD_TIMEOUT: return "device wait timed out";
         case TBMD_NO_DEVICE: return "no sm_100 CUDA device";
+        case TBMD_TOO_LARGE: return "n above the allocation-free limit";
     }
     return "unknown status";
 }
