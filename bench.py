@@ -186,7 +186,9 @@ def run_ours(args, world, rank, local):
 
     w = WORKLOADS[args.workload]
     torch.cuda.set_device(local)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library, the CUDA events and the L2 flush all run on it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     st = make_input(w)
     n = len(st["x"])
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")

@@ -62,7 +62,8 @@ typedef struct {
     double nu;          /* AT strength; the reference uses AxilrodTeller(1.0) (main.cpp:41,66,91) */
     int32_t device;     /* CUDA device ordinal */
     int32_t use_graph;  /* 1: capture multi-step runs in a CUDA graph */
-    void *stream;       /* cudaStream_t to run on, or NULL for a stream owned by the context */
+    void *stream;       /* cudaStream_t to run on, or NULL for a non-blocking stream owned by the
+                           context (multi-step graphs need a stream that is not the legacy default) */
     int32_t reserved[8];
 } tbmd_config;
 
@@ -112,7 +113,9 @@ tbmd_status tbmd_adjoint(tbmd_ctx *ctx, const double *gfx, const double *gfy, co
                          double *gx, double *gy, double *gz, double *g_nu);
 
 /* Device-pointer variants for callers that already hold device memory (torch tensors).  They run
- * asynchronously on `stream` (cudaStream_t; NULL = the context stream) with positions of length n
+ * asynchronously on `stream` (cudaStream_t; NULL = the context stream, which is a non-blocking
+ * stream: pass cudaStreamLegacy, i.e. (void *)1, to order with the legacy default stream, which
+ * torch reports as handle 0) with positions of length n
  * given by the caller; the context's P3BCA domain is used (set it first with tbmd_set_domain or
  * tbmd_set_particles).  energy and triplets are device scalars (may be NULL). */
 tbmd_status tbmd_forces_device(tbmd_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,

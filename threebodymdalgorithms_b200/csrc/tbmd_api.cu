@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 #include <new>
 #include <string>
@@ -70,6 +71,7 @@ struct tbmd_ctx {
 
     // no-cutoff sweeps
     int R_auta = 4, R_nata = 2, R_fp64 = 2;
+    DevBuf sweep_sys;  // single system: sys_items[2], sys_off[2], sys_prefix[1], sys_nblocks[1]
     DevBuf prefix;
     int prefix_JB = 0, prefix_alg = -1;
     int64_t prefix_n = -1;
@@ -81,7 +83,10 @@ struct tbmd_ctx {
     // P3BCA
     bool domain_set = false;
     double L[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
-    Grid grid{};
+    Grid grid{};          // single system, or for a batch: first system's grid with ncells = all cells
+    GridSet gset{};       // device tables of the systems being evaluated
+    DevBuf gset_single;   // Grid[1] + cell_off[2] + sys_off[2] of the single-system case
+    int max_stage = 256;  // neighbour staging capacity
     DevBuf cell_n, cell_c, nbr_buf;
     int64_t cell_bufs_n = -1, cell_bufs_cells = -1;
     CellBufs cb{};
@@ -91,6 +96,9 @@ struct tbmd_ctx {
 
     // adjoint / device-variant scratch
     DevBuf dirs, hvp;
+
+    // batched evaluation (tbmd_batch_*): packed positions/directions/outputs and system tables
+    DevBuf bpos, bout, bsys, bprefix;
 
     // phase profiling (eager mode): marks recorded on the stream, resolved after each sync
     bool profiling = false;
@@ -213,6 +221,14 @@ static tbmd_status ensure_sweep(tbmd_ctx *ctx, int alg, int64_t n, int R, bool d
         ctx->prefix_alg = alg;
         ctx->nblocks = (int)nb;
         ctx->total_items = total;
+        // one system: sys_items = {0, total}, sys_off = {0, n}, sys_prefix = {0}, sys_nblocks = {nb}
+        struct {
+            int64_t items[2], off[2], pre[1];
+            int32_t nbl[2];
+        } tab = {{0, total}, {0, n}, {0}, {(int32_t)nb, 0}};
+        CK(ctx->sweep_sys.ensure(sizeof tab));
+        CK(cudaMemcpyAsync(ctx->sweep_sys.p, &tab, sizeof tab, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
         if (alg == TBMD_NATA) CK(ctx->partial.ensure(sizeof(double) * 3 * (size_t)n * (size_t)(nb > 0 ? nb : 1)));
     }
     int per_sm = 0, sms = 0;
@@ -222,6 +238,15 @@ static tbmd_status ensure_sweep(tbmd_ctx *ctx, int alg, int64_t n, int R, bool d
     if (per_sm < 1) per_sm = 1;
     ctx->sweep_grid = sms * per_sm;
     return TBMD_OK;
+}
+
+// Work list of the single system of the context (tables filled by ensure_sweep).
+static SweepWork single_sweep(tbmd_ctx *ctx)
+{
+    const char *t = ctx->sweep_sys.as<char>();
+    return SweepWork{ctx->prefix.as<int64_t>(), ctx->nblocks, ctx->total_items, sweep_counter(ctx), 1,
+                     (const int64_t *)t, (const int64_t *)(t + 16), (const int64_t *)(t + 32),
+                     (const int32_t *)(t + 40)};
 }
 
 // Cell grid for the current domain and cutoff (oracle tbo_cell_dims).
@@ -238,6 +263,25 @@ static void make_grid(tbmd_ctx *ctx)
     }
     g.ncells = (int64_t)g.dims[0] * g.dims[1] * g.dims[2];
     g.sqcut = ctx->cfg.cutoff * ctx->cfg.cutoff;
+    fill_grid_test_params(g);
+}
+
+// Grid of one system from its box (L, lo) and the context's cutoff (same rule as make_grid).
+static Grid system_grid(const tbmd_ctx *ctx, const double *L, const double *lo)
+{
+    Grid g{};
+    for (int d = 0; d < 3; ++d) {
+        double m = std::floor(L[d] / (ctx->cfg.cutoff * kCellMargin));
+        int nd = (m >= 3.0) ? (m > 1024.0 ? 1024 : (int)m) : 1;
+        g.dims[d] = nd;
+        g.L[d] = L[d];
+        g.lo[d] = lo[d];
+        g.w[d] = L[d] / (double)nd;
+    }
+    g.ncells = (int64_t)g.dims[0] * g.dims[1] * g.dims[2];
+    g.sqcut = ctx->cfg.cutoff * ctx->cfg.cutoff;
+    fill_grid_test_params(g);
+    return g;
 }
 
 // Neighbour-list capacity estimate from the mean density: twice the expected half-list length
@@ -254,13 +298,10 @@ static int initial_cap(const tbmd_ctx *ctx, int64_t n)
     return cap < 32 ? 32 : cap;
 }
 
-static tbmd_status ensure_cells(tbmd_ctx *ctx, int64_t n, bool dual, bool energy)
+// Cell-grid buffers for n particles and ncells cells (all systems), neighbour lists at ctx->cap,
+// and the triplet kernel's launch plan.
+static tbmd_status ensure_cell_bufs(tbmd_ctx *ctx, int64_t n, int64_t nc, bool dual, bool energy)
 {
-    if (!ctx->domain_set)
-        return fail(ctx, TBMD_NOT_READY, "P3BCA needs a domain: set particles or call tbmd_set_domain");
-    make_grid(ctx);
-    const int64_t nc = ctx->grid.ncells;
-    if (ctx->cap == 0) ctx->cap = initial_cap(ctx, n);
     if (ctx->cell_bufs_n != n || ctx->cell_bufs_cells != nc) {
         // per particle: FP64 xs ys zs dxs dys dzs fs[3] hs[3]; int32 cell_of, sorted, nbr_count
         CK(ctx->cell_n.ensure((size_t)n * (12 * sizeof(double) + 3 * sizeof(int32_t)) + 256));
@@ -297,6 +338,26 @@ static tbmd_status ensure_cells(tbmd_ctx *ctx, int64_t n, bool dual, bool energy
     return TBMD_OK;
 }
 
+static tbmd_status ensure_cells(tbmd_ctx *ctx, int64_t n, bool dual, bool energy)
+{
+    if (!ctx->domain_set)
+        return fail(ctx, TBMD_NOT_READY, "P3BCA needs a domain: set particles or call tbmd_set_domain");
+    make_grid(ctx);
+    if (ctx->cap == 0) ctx->cap = initial_cap(ctx, n);
+    // single-system tables: grids[0], cell_off = {0, ncells}, sys_off = {0, n}
+    struct {
+        Grid g;
+        int64_t cell_off[2], sys_off[2];
+    } tab = {ctx->grid, {0, ctx->grid.ncells}, {0, n}};
+    CK(ctx->gset_single.ensure(sizeof tab));
+    CK(cudaMemcpyAsync(ctx->gset_single.p, &tab, sizeof tab, cudaMemcpyHostToDevice, ctx->stream));
+    char *base = ctx->gset_single.as<char>();
+    ctx->gset = GridSet{(const Grid *)base, (const int64_t *)(base + offsetof(decltype(tab), cell_off)),
+                        (const int64_t *)(base + offsetof(decltype(tab), sys_off)), 1};
+    ctx->max_stage = neighbor_stage_cap(ctx->grid, n);
+    return ensure_cell_bufs(ctx, n, ctx->grid.ncells, dual, energy);
+}
+
 static tbmd_status ensure_scalars(tbmd_ctx *ctx)
 {
     if (!ctx->scalars.p) {
@@ -330,16 +391,16 @@ static tbmd_status enqueue_forces(tbmd_ctx *ctx, int64_t n, Pos pos, Out out, bo
     if (is_p3bca_cut(ctx)) {
         CellBufs &cb = ctx->cb;
         phase_mark(ctx, st, PH_CELLS, *nl);
-        CK(launch_cell_build(n, pos, ctx->grid, cb, dual, st, nl));
+        CK(launch_cell_build(n, pos, ctx->grid, ctx->gset, cb, dual, st, nl));
         phase_mark(ctx, st, PH_NEIGHBORS, *nl);
-        CK(launch_neighbors(n, ctx->grid, cb, st));
+        CK(launch_neighbors(n, ctx->grid, ctx->gset, ctx->max_stage, cb, st));
         *nl += 1;
         for (int k = 0; k < 3; ++k) {
             CK(cudaMemsetAsync(cb.fs[k], 0, sizeof(double) * n, st));
             if (dual) CK(cudaMemsetAsync(cb.hs[k], 0, sizeof(double) * n, st));
         }
         phase_mark(ctx, st, PH_TRIPLETS, *nl);
-        CK(launch_p3bca(mx, dual, energy != nullptr, n, ctx->grid, cb, nu, energy, count, ctx->plan, st));
+        CK(launch_p3bca(mx, dual, energy != nullptr, n, ctx->grid, ctx->gset, cb, nu, energy, count, ctx->plan, st));
         *nl += 1;
         phase_mark(ctx, st, PH_UPDATE, *nl);
         CK(launch_unsort(n, cb, out, dual, st));
@@ -347,7 +408,7 @@ static tbmd_status enqueue_forces(tbmd_ctx *ctx, int64_t n, Pos pos, Out out, bo
         return TBMD_OK;
     }
     phase_mark(ctx, st, PH_TRIPLETS, *nl);
-    SweepWork w{ctx->prefix.as<int64_t>(), ctx->nblocks, ctx->total_items, sweep_counter(ctx)};
+    SweepWork w = single_sweep(ctx);
     CK(cudaMemsetAsync(w.counter, 0, sizeof(unsigned int), st));
     if (ctx->cfg.algorithm == TBMD_NATA && !dual) {
         CK(launch_nata(mx, false, ctx->prefix_JB / 32, energy != nullptr, n, pos, out, energy, nu, w,
@@ -520,7 +581,8 @@ void tbmd_destroy(tbmd_ctx *ctx)
     for (auto &m : ctx->marks) cudaEventDestroy(m.second);
     for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
     for (DevBuf *b : {&ctx->state, &ctx->snapshot, &ctx->scalars, &ctx->step_counts, &ctx->prefix, &ctx->partial,
-                      &ctx->cell_n, &ctx->cell_c, &ctx->nbr_buf, &ctx->dirs, &ctx->hvp})
+                      &ctx->cell_n, &ctx->cell_c, &ctx->nbr_buf, &ctx->dirs, &ctx->hvp, &ctx->gset_single,
+                      &ctx->sweep_sys, &ctx->bpos, &ctx->bout, &ctx->bsys, &ctx->bprefix})
         b->release();
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -827,7 +889,7 @@ tbmd_status tbmd_cells(tbmd_ctx *ctx, int32_t *cell_of_particle, int32_t *dims, 
         st = ensure_cells(ctx, ctx->n, false, false);
         if (st != TBMD_OK) return st;
         int nl = 0;
-        CK(launch_cell_build(ctx->n, state_pos(ctx), ctx->grid, ctx->cb, false, ctx->stream, &nl));
+        CK(launch_cell_build(ctx->n, state_pos(ctx), ctx->grid, ctx->gset, ctx->cb, false, ctx->stream, &nl));
         ctx->launches += nl;
         CK(cudaMemcpyAsync(cell_of_particle, ctx->cb.cell_of, sizeof(int32_t) * ctx->n, cudaMemcpyDeviceToHost,
                            ctx->stream));
@@ -985,17 +1047,247 @@ extern "C" tbmd_status tbmd_autotune(tbmd_ctx *ctx, const char *cache_path)
     return TBMD_OK;
 }
 
-extern "C" tbmd_status tbmd_batch_forces(tbmd_ctx *ctx, int32_t, const int64_t *, const double *, const double *,
-                                         const double *, const double *, const double *, double *, double *, double *,
-                                         double *, uint64_t *)
+// ---------------------------------------------------------------------------------------------
+// Batched evaluation: nsys independent systems packed back to back, each with its own P3BCA
+// domain, evaluated together: one sweep launch over all systems (no cutoff), or one cell build,
+// one neighbour pass and one triplet launch over all systems (P3BCA).
+
+struct BatchResult {
+    std::vector<double> f, h;       // 3 * N each (h only for the adjoint)
+    std::vector<double> energy;     // nsys
+    std::vector<uint64_t> counts;   // nsys
+};
+
+static tbmd_status batch_eval(tbmd_ctx *ctx, int32_t nsys, const int64_t *offsets, const double *box,
+                              const double *lo, const double *x, const double *y, const double *z, const double *gfx,
+                              const double *gfy, const double *gfz, BatchResult &res)
 {
-    return fail(ctx, TBMD_INVALID_ARG, "batched evaluation is not built yet");
+    if (!ctx || !offsets || !x || !y || !z) return TBMD_INVALID_ARG;
+    if (nsys < 1) return fail(ctx, TBMD_INVALID_ARG, "nsys < 1");
+    if (offsets[0] != 0) return fail(ctx, TBMD_INVALID_ARG, "offsets[0] must be 0");
+    for (int s = 0; s < nsys; ++s)
+        if (offsets[s + 1] < offsets[s]) return fail(ctx, TBMD_INVALID_ARG, "offsets must not decrease");
+    const int64_t N = offsets[nsys];
+    if (N < 1 || N > (int64_t)INT32_MAX / 2) return fail(ctx, TBMD_INVALID_ARG, "total n out of range");
+    for (const double *a : {x, y, z})
+        if (!finite3(a, N)) return fail(ctx, TBMD_BAD_INPUT, "non-finite position");
+    const bool dual = gfx != nullptr;
+    tbmd_status st = check_device(ctx);
+    if (st != TBMD_OK) return st;
+    st = ensure_scalars(ctx);
+    if (st != TBMD_OK) return st;
+    CK(cudaStreamSynchronize(ctx->stream));
+    invalidate_graph(ctx);
+    const bool mx = mixed(ctx);
+    const double nu = ctx->cfg.nu == 0.0 ? 1.0 : ctx->cfg.nu;  // nu = 0: evaluate the nu = 1 parts
+    cudaStream_t sm = ctx->stream;
+
+    // positions (+ direction) and outputs (f, h, energy[nsys], counts[nsys])
+    CK(ctx->bpos.ensure(sizeof(double) * 6 * (size_t)N));
+    double *P = ctx->bpos.as<double>();
+    CK(cudaMemcpyAsync(P, x, sizeof(double) * N, cudaMemcpyHostToDevice, sm));
+    CK(cudaMemcpyAsync(P + N, y, sizeof(double) * N, cudaMemcpyHostToDevice, sm));
+    CK(cudaMemcpyAsync(P + 2 * N, z, sizeof(double) * N, cudaMemcpyHostToDevice, sm));
+    if (dual) {
+        CK(cudaMemcpyAsync(P + 3 * N, gfx, sizeof(double) * N, cudaMemcpyHostToDevice, sm));
+        CK(cudaMemcpyAsync(P + 4 * N, gfy, sizeof(double) * N, cudaMemcpyHostToDevice, sm));
+        CK(cudaMemcpyAsync(P + 5 * N, gfz, sizeof(double) * N, cudaMemcpyHostToDevice, sm));
+    }
+    CK(ctx->bout.ensure(sizeof(double) * (6 * (size_t)N + 2 * (size_t)nsys)));
+    double *O = ctx->bout.as<double>();
+    double *E = O + 6 * N;
+    unsigned long long *CNT = (unsigned long long *)(E + nsys);
+    CK(cudaMemsetAsync(E, 0, sizeof(double) * 2 * nsys, sm));
+    const Pos pos{P, P + N, P + 2 * N, dual ? P + 3 * N : nullptr, dual ? P + 4 * N : nullptr,
+                  dual ? P + 5 * N : nullptr};
+    const Out out{O, O + N, O + 2 * N, O + 3 * N, O + 4 * N, O + 5 * N};
+    res.counts.assign(nsys, 0);
+    int nl = 0;
+
+    if (is_p3bca_cut(ctx)) {
+        // per-system grids: the given box, or the reference's domain rule on that system's positions
+        std::vector<Grid> grids(nsys);
+        std::vector<int64_t> cell_off(nsys + 1, 0);
+        int cap = 32, stage = 256;
+        for (int s = 0; s < nsys; ++s) {
+            double Ls[3], los[3];
+            const int64_t b = offsets[s], e = offsets[s + 1];
+            for (int d = 0; d < 3; ++d) {
+                if (box) {
+                    Ls[d] = box[3 * s + d];
+                    los[d] = lo ? lo[3 * s + d] : 0.0;
+                } else {
+                    const double *p = d == 0 ? x : (d == 1 ? y : z);
+                    double mn = e > b ? p[b] : 0.0, mxv = mn;
+                    for (int64_t i = b; i < e; ++i) {
+                        mn = p[i] < mn ? p[i] : mn;
+                        mxv = p[i] > mxv ? p[i] : mxv;
+                    }
+                    los[d] = mn - 0.0001;
+                    Ls[d] = std::fabs((mxv + 0.0001) - los[d]);
+                }
+                if (!(Ls[d] > 0) || !std::isfinite(Ls[d]) || !std::isfinite(los[d]))
+                    return fail(ctx, TBMD_INVALID_ARG, "bad box of system %d", s);
+            }
+            grids[s] = system_grid(ctx, Ls, los);
+            cell_off[s + 1] = cell_off[s] + grids[s].ncells;
+            const double vol = Ls[0] * Ls[1] * Ls[2], c = ctx->cfg.cutoff;
+            const double half = 4.18879020478639 * c * c * c * ((double)(e - b) / vol) * 0.5;
+            int want = ((int)(2.0 * half + 48.0) + 31) / 32 * 32;
+            cap = want > cap ? want : cap;
+            const int sc = neighbor_stage_cap(grids[s], e - b);
+            stage = sc > stage ? sc : stage;
+        }
+        const size_t gbytes = sizeof(Grid) * nsys, obytes = sizeof(int64_t) * (nsys + 1);
+        CK(ctx->bsys.ensure(gbytes + 2 * obytes + 64));
+        char *tb = ctx->bsys.as<char>();
+        CK(cudaMemcpyAsync(tb, grids.data(), gbytes, cudaMemcpyHostToDevice, sm));
+        CK(cudaMemcpyAsync(tb + gbytes, cell_off.data(), obytes, cudaMemcpyHostToDevice, sm));
+        CK(cudaMemcpyAsync(tb + gbytes + obytes, offsets, obytes, cudaMemcpyHostToDevice, sm));
+        const int saved_cap = ctx->cap;
+        Grid all = grids[0];
+        all.ncells = cell_off[nsys];
+        ctx->cap = cap;
+        tbmd_status r = TBMD_CAPACITY_RETRY;
+        for (int attempt = 0; attempt < 4; ++attempt) {
+            ctx->grid = all;
+            ctx->gset = GridSet{(const Grid *)tb, (const int64_t *)(tb + gbytes), (const int64_t *)(tb + gbytes + obytes),
+                                nsys};
+            ctx->max_stage = stage;
+            r = ensure_cell_bufs(ctx, N, all.ncells, dual, true);
+            if (r != TBMD_OK) break;
+            CK(cudaMemsetAsync(ctx->scalars.as<char>() + 28, 0, 4, sm));
+            CK(cudaMemsetAsync(E, 0, sizeof(double) * 2 * nsys, sm));
+            CellBufs &cb = ctx->cb;
+            CK(launch_cell_build(N, pos, ctx->grid, ctx->gset, cb, dual, sm, &nl));
+            CK(launch_neighbors(N, ctx->grid, ctx->gset, ctx->max_stage, cb, sm));
+            for (int k = 0; k < 3; ++k) {
+                CK(cudaMemsetAsync(cb.fs[k], 0, sizeof(double) * N, sm));
+                if (dual) CK(cudaMemsetAsync(cb.hs[k], 0, sizeof(double) * N, sm));
+            }
+            CK(launch_p3bca(mx, dual, true, N, ctx->grid, ctx->gset, cb, nu, E, CNT, ctx->plan, sm));
+            CK(launch_unsort(N, cb, out, dual, sm));
+            nl += 3 + (dual ? 1 : 0);
+            int32_t seen = 0;
+            CK(cudaMemcpyAsync(&seen, ctx->scalars.as<char>() + 28, sizeof seen, cudaMemcpyDeviceToHost, sm));
+            CK(cudaStreamSynchronize(sm));
+            r = TBMD_OK;
+            if (!grow_cap(ctx, seen)) break;
+            r = TBMD_CAPACITY_RETRY;
+        }
+        ctx->cap = saved_cap > ctx->cap ? saved_cap : ctx->cap;  // the next ensure_cells rebuilds the single grid
+        if (r != TBMD_OK) return r == TBMD_CAPACITY_RETRY ? fail(ctx, r, "neighbour capacity exceeded") : r;
+        std::vector<unsigned long long> c(nsys);
+        CK(cudaMemcpyAsync(c.data(), CNT, sizeof(unsigned long long) * nsys, cudaMemcpyDeviceToHost, sm));
+        CK(cudaStreamSynchronize(sm));
+        for (int s = 0; s < nsys; ++s) res.counts[s] = c[s];
+    } else {
+        // one sweep over all systems (AUTA work items; NATA gives the same forces)
+        const int R = dual ? (mx ? 2 : 1) : (mx ? ctx->R_auta : ctx->R_fp64);
+        const int JB = 32 * R;
+        std::vector<int64_t> prefix, sys_items(nsys + 1, 0), sys_prefix(nsys, 0);
+        std::vector<int32_t> sys_nb(nsys, 0);
+        for (int s = 0; s < nsys; ++s) {
+            const int64_t ns = offsets[s + 1] - offsets[s];
+            const int64_t nb = ns >= 3 ? (ns - 2 + JB) / JB : 0;
+            std::vector<int64_t> pre((size_t)nb + 1, 0);
+            const int64_t items = sweep_items(TBMD_AUTA, ns, JB, pre.data());
+            sys_prefix[s] = (int64_t)prefix.size();
+            sys_nb[s] = (int32_t)nb;
+            prefix.insert(prefix.end(), pre.begin(), pre.end());
+            sys_items[s + 1] = sys_items[s] + items;
+            res.counts[s] = choose3(ns);
+        }
+        if (sys_items[nsys] >= (int64_t)UINT32_MAX - 65536) return fail(ctx, TBMD_INVALID_ARG, "too many work items");
+        const size_t pb = sizeof(int64_t) * prefix.size();
+        CK(ctx->bprefix.ensure(pb + 64));
+        CK(cudaMemcpyAsync(ctx->bprefix.p, prefix.data(), pb, cudaMemcpyHostToDevice, sm));
+        const size_t ib = sizeof(int64_t) * (nsys + 1), nbb = sizeof(int32_t) * nsys;
+        CK(ctx->bsys.ensure(3 * ib + nbb + 64));
+        char *tb = ctx->bsys.as<char>();
+        CK(cudaMemcpyAsync(tb, sys_items.data(), ib, cudaMemcpyHostToDevice, sm));
+        CK(cudaMemcpyAsync(tb + ib, offsets, ib, cudaMemcpyHostToDevice, sm));
+        CK(cudaMemcpyAsync(tb + 2 * ib, sys_prefix.data(), sizeof(int64_t) * nsys, cudaMemcpyHostToDevice, sm));
+        CK(cudaMemcpyAsync(tb + 3 * ib, sys_nb.data(), nbb, cudaMemcpyHostToDevice, sm));
+        SweepWork w{ctx->bprefix.as<int64_t>(), 0, sys_items[nsys], sweep_counter(ctx), nsys, (const int64_t *)tb,
+                    (const int64_t *)(tb + ib), (const int64_t *)(tb + 2 * ib), (const int32_t *)(tb + 3 * ib)};
+        CK(cudaMemsetAsync(O, 0, sizeof(double) * (dual ? 6 : 3) * N, sm));
+        CK(cudaMemsetAsync(w.counter, 0, sizeof(unsigned int), sm));
+        int sms = 0;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+        CK(launch_auta(mx, dual, R, true, N, pos, out, E, nu, w, sms * 8, sm));
+        nl += 1;
+    }
+    ctx->launches += nl;
+    res.f.resize(3 * N);
+    res.energy.resize(nsys);
+    CK(cudaMemcpyAsync(res.f.data(), O, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, sm));
+    if (dual) {
+        res.h.resize(3 * N);
+        CK(cudaMemcpyAsync(res.h.data(), O + 3 * N, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, sm));
+    }
+    CK(cudaMemcpyAsync(res.energy.data(), E, sizeof(double) * nsys, cudaMemcpyDeviceToHost, sm));
+    CK(cudaStreamSynchronize(sm));
+    if (ctx->cfg.nu == 0.0) {  // the nu = 1 parts were evaluated; the true f, E and H vanish
+        for (double &v : res.f) v = 0.0;
+        for (double &v : res.h) v = 0.0;
+        for (double &v : res.energy) v = 0.0;
+    }
+    return TBMD_OK;
 }
 
-extern "C" tbmd_status tbmd_batch_adjoint(tbmd_ctx *ctx, int32_t, const int64_t *, const double *, const double *,
-                                          const double *, const double *, const double *, const double *,
-                                          const double *, const double *, const double *, double *, double *, double *,
-                                          double *)
+extern "C" tbmd_status tbmd_batch_forces(tbmd_ctx *ctx, int32_t nsys, const int64_t *offsets, const double *box,
+                                         const double *lo, const double *x, const double *y, const double *z,
+                                         double *fx, double *fy, double *fz, double *energy, uint64_t *triplets)
 {
-    return fail(ctx, TBMD_INVALID_ARG, "batched evaluation is not built yet");
+    BatchResult r;
+    tbmd_status st = batch_eval(ctx, nsys, offsets, box, lo, x, y, z, nullptr, nullptr, nullptr, r);
+    if (st != TBMD_OK) return st;
+    const int64_t N = offsets[nsys];
+    double *o3[3] = {fx, fy, fz};
+    for (int k = 0; k < 3; ++k)
+        if (o3[k]) std::memcpy(o3[k], r.f.data() + k * N, sizeof(double) * N);
+    for (int s = 0; s < nsys; ++s) {
+        if (energy) energy[s] = r.energy[s];
+        if (triplets) triplets[s] = r.counts[s];
+    }
+    return TBMD_OK;
+}
+
+extern "C" tbmd_status tbmd_batch_adjoint(tbmd_ctx *ctx, int32_t nsys, const int64_t *offsets, const double *box,
+                                          const double *lo, const double *x, const double *y, const double *z,
+                                          const double *gfx, const double *gfy, const double *gfz,
+                                          const double *g_energy, double *gx, double *gy, double *gz, double *g_nu)
+{
+    if (!gfx || !gfy || !gfz || !g_energy) return ctx ? fail(ctx, TBMD_INVALID_ARG, "null cotangent") : TBMD_INVALID_ARG;
+    BatchResult r;
+    tbmd_status st = batch_eval(ctx, nsys, offsets, box, lo, x, y, z, gfx, gfy, gfz, r);
+    if (st != TBMD_OK) return st;
+    const int64_t N = offsets[nsys];
+    const double *g3[3] = {gfx, gfy, gfz};
+    double *o3[3] = {gx, gy, gz};
+    const double nu = ctx->cfg.nu;
+    std::vector<double> fe(3 * N, 0.0);
+    // with nu = 0 batch_eval zeroed f, E and H; g_nu needs the nu = 1 parts, recomputed below
+    if (nu == 0.0) {
+        BatchResult r1;
+        ctx->cfg.nu = 1.0;
+        st = batch_eval(ctx, nsys, offsets, box, lo, x, y, z, nullptr, nullptr, nullptr, r1);
+        ctx->cfg.nu = 0.0;
+        if (st != TBMD_OK) return st;
+        r.f.swap(r1.f);
+        r.energy.swap(r1.energy);
+    }
+    for (int s = 0; s < nsys; ++s) {
+        const double ge = g_energy[s];
+        if (!std::isfinite(ge)) return fail(ctx, TBMD_INVALID_ARG, "g_energy of system %d not finite", s);
+        double dot = 0.0;
+        for (int k = 0; k < 3; ++k)
+            for (int64_t i = offsets[s]; i < offsets[s + 1]; ++i) {
+                dot += g3[k][i] * r.f[k * N + i];
+                if (o3[k]) o3[k][i] = nu == 0.0 ? 0.0 : r.h[k * N + i] + ge * r.f[k * N + i];
+            }
+        if (g_nu) g_nu[s] = nu == 0.0 ? dot + ge * r.energy[s] : (dot + ge * r.energy[s]) / nu;
+    }
+    return TBMD_OK;
 }

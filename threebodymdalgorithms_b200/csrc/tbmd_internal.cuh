@@ -193,27 +193,48 @@ struct Pos {
     const double *dx, *dy, *dz;
 };
 
-// Static work list of the no-cutoff sweeps.  A work item is (block b of JB consecutive j, i).
+// Static work list of the no-cutoff sweeps.  A work item is (system, block b of JB consecutive j,
+// i).  Systems are packed back to back (particles sys_off[s] .. sys_off[s+1]-1); a single system
+// is nsys = 1.  NATA uses only nblocks/total/counter (its items are b * n + i).
 struct SweepWork {
-    const int64_t *prefix;  // items of blocks < b, nblocks + 1 entries
-    int nblocks;
-    int64_t total;
-    unsigned int *counter;  // dynamic item counter, zeroed before the launch
+    const int64_t *prefix;       // per system: items of blocks < b (nblocks_s + 1 entries each)
+    int nblocks;                 // single-system NATA: number of j-blocks
+    int64_t total;               // items over all systems
+    unsigned int *counter;       // dynamic item counter, zeroed before the launch
+    int nsys;
+    const int64_t *sys_items;    // [nsys + 1] first item of each system
+    const int64_t *sys_off;      // [nsys + 1] first particle of each system
+    const int64_t *sys_prefix;   // [nsys] start of each system's block prefix in `prefix`
+    const int32_t *sys_nblocks;  // [nsys]
 };
 
-// Cell grid of the P3BCA path.
+// Cell grid of the P3BCA path (one per system).  band/raw_ok parametrise the mixed cutoff test.
 struct Grid {
     double L[3], lo[3], w[3];
     int dims[3];
     int64_t ncells;
     double sqcut;
+    float band;   // half-width of the FP32 uncertainty band around cutoff^2
+    int raw_ok;   // every box length >= 4 cutoffs: raw distance = periodic formula for non-wrapping pairs
 };
+
+// Several independent systems packed back to back: system s owns particles (and sorted slots)
+// sys_off[s] .. sys_off[s+1]-1 and cells cell_off[s] .. cell_off[s+1]-1 of the concatenated grid.
+// nsys = 1 is the single-system case (the kernels then use the Grid passed by value).
+struct GridSet {
+    const Grid *grids;       // [nsys] device
+    const int64_t *cell_off;  // [nsys + 1] device
+    const int64_t *sys_off;   // [nsys + 1] device
+    int nsys;
+};
+void fill_grid_test_params(Grid &g);
 
 // ---------------------------------------------------------------------------------------------
 // Launchers (tbmd_kernels.cu).  All take the stream they run on and return the launch error.
 
 int sweep_block_size(int algorithm, bool mixed, bool dual, int R);
 int64_t sweep_items(int algorithm, int64_t n, int JB, int64_t *prefix_host /* nb+1 or NULL */);
+// energy_out: one accumulator per system (index = system)
 
 cudaError_t launch_auta(bool mixed, bool dual, int R, bool energy, int64_t n, Pos pos, Out out, double *energy_out,
                         double nu, SweepWork work, int grid, cudaStream_t st);
@@ -238,9 +259,12 @@ struct CellBufs {
     double *fs[3];         // [n] forces in sorted order
     double *hs[3];         // [n] H*direction in sorted order (adjoint)
 };
-cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, CellBufs &cb, bool with_dir, cudaStream_t st,
-                              int *launches);
-cudaError_t launch_neighbors(int64_t n, const Grid &g, CellBufs &cb, cudaStream_t st);
+// For a GridSet, g is the first system's grid with ncells = total cells over all systems.
+cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, const GridSet &set, CellBufs &cb, bool with_dir,
+                              cudaStream_t st, int *launches);
+cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, int max_stage, CellBufs &cb,
+                             cudaStream_t st);
+int neighbor_stage_cap(const Grid &g, int64_t n);
 // Launch shape of the P3BCA triplet kernel for a list capacity; computed outside graph capture.
 struct P3Plan {
     int warps = 0;
@@ -248,8 +272,10 @@ struct P3Plan {
     int grid = 0;
 };
 cudaError_t plan_p3bca(bool mixed, bool dual, bool energy, int cap, int warps_requested, P3Plan *plan);
-cudaError_t launch_p3bca(bool mixed, bool dual, bool energy, int64_t n, const Grid &g, CellBufs &cb, double nu,
-                         double *energy_out, unsigned long long *count_out, const P3Plan &plan, cudaStream_t st);
+// energy_out / count_out: one accumulator per system
+cudaError_t launch_p3bca(bool mixed, bool dual, bool energy, int64_t n, const Grid &g, const GridSet &set,
+                         CellBufs &cb, double nu, double *energy_out, unsigned long long *count_out,
+                         const P3Plan &plan, cudaStream_t st);
 // forces (and H*d) from sorted order back to input order
 cudaError_t launch_unsort(int64_t n, const CellBufs &cb, Out out, bool dual, cudaStream_t st);
 

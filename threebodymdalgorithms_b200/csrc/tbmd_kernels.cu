@@ -134,7 +134,6 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const S nu = constant<S>(nu_d), nu3 = constant<S>(-3.0 * nu_d), nu15 = constant<S>(15.0 * nu_d);
-    Acc en_acc = to_acc(szero<S>());
 
     unsigned int w = 0;
     if (lane == 0) w = atomicAdd(work.counter, 1u);
@@ -142,8 +141,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
     while ((int64_t)w < work.total) {
         unsigned int wn = 0;
         if (lane == 0) wn = atomicAdd(work.counter, 1u);
-        const int b = find_block(work.prefix, work.nblocks, (int64_t)w);
-        const int64_t i = (int64_t)w - work.prefix[b];
+        // system, then (block, i) inside it
+        const int sys = work.nsys > 1 ? find_block(work.sys_items, work.nsys, (int64_t)w) : 0;
+        const int64_t wl = (int64_t)w - work.sys_items[sys];
+        const int64_t off = work.sys_off[sys], hi = work.sys_off[sys + 1];
+        const int64_t *prefix = work.prefix + work.sys_prefix[sys];
+        const int b = find_block(prefix, work.sys_nblocks[sys], wl);
+        const int64_t i = off + wl - prefix[b];
         const double xi = pos.x[i], yi = pos.y[i], zi = pos.z[i];
         double dxi = 0.0, dyi = 0.0, dzi = 0.0;
         if (Traits<S>::dual) {
@@ -158,8 +162,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
         V3<Acc> fj[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            jj[r] = (int64_t)b * JB + r * 32 + lane;
-            jv[r] = jj[r] > i && jj[r] < n;
+            jj[r] = off + (int64_t)b * JB + r * 32 + lane;
+            jv[r] = jj[r] > i && jj[r] < hi;
             u[r] = vzero<S>();
             ul[r] = vzero<S>();
             if (jv[r]) edge<S>(pos, jj[r], xi, yi, zi, dxi, dyi, dzi, u[r], ul[r]);
@@ -167,9 +171,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
             fj[r] = widen(vzero<S>());
         }
         V3<Acc> fi = widen(vzero<S>());
-        for (int64_t kt = (int64_t)b * JB; kt < n; kt += 32) {
+        Acc en_item = to_acc(szero<S>());
+        for (int64_t kt = off + (int64_t)b * JB; kt < hi; kt += 32) {
             const int64_t k = kt + lane;
-            const bool kv = k < n;
+            const bool kv = k < hi;
             V3<S> vk = vzero<S>(), vkl = vzero<S>();
             if (kv) edge<S>(pos, k, xi, yi, zi, dxi, dyi, dzi, vk, vkl);
             {
@@ -201,7 +206,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
                 const int64_t kidx = kt + kk;
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    const bool valid = jv[r] && kidx > jj[r] && kidx < n;
+                    const bool valid = jv[r] && kidx > jj[r] && kidx < hi;
                     const ATCoef<S> cf = triplet<ENERGY>(u[r], ul[r], aa[r], v, vl, e.b, nu, nu3, nu15, valid, en);
                     al[r] = al[r] + cf.alpha;
                     gv[r] = fma3(v, cf.gamma, gv[r]);
@@ -222,7 +227,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
                 fj[r] = fj[r] + f;
                 fi = fi - f;
             }
-            if (ENERGY) en_acc = en_acc + to_acc(en);
+            if (ENERGY) en_item = en_item + to_acc(en);
             __syncwarp();
         }
 #pragma unroll
@@ -230,11 +235,11 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
             if (jv[r]) atomic_out(out, jj[r], fj[r]);
         fi = warp_sum3(fi);
         if (lane == 0) atomic_out(out, i, fi);
+        if (ENERGY) {
+            en_item = warp_sum(en_item);
+            if (lane == 0) atomicAdd(energy_out + sys, acc_value(en_item));
+        }
         w = __shfl_sync(0xffffffffu, wn, 0);
-    }
-    if (ENERGY) {
-        en_acc = warp_sum(en_acc);
-        if (lane == 0) atomicAdd(energy_out, acc_value(en_acc));
     }
 }
 
@@ -471,16 +476,24 @@ __device__ __forceinline__ double sqdist_periodic(double xa, double ya, double z
     return __dadd_rn(__dadd_rn(__dmul_rn(mx, mx), __dmul_rn(my, my)), __dmul_rn(mz, mz));
 }
 
+// index of the system owning item idx (sys_off has nsys + 1 entries)
+__device__ __forceinline__ int system_of(const int64_t *sys_off, int nsys, int64_t idx)
+{
+    return nsys > 1 ? find_block(sys_off, nsys, idx) : 0;
+}
+
 __global__ void k_cell_assign(int64_t n, const double *__restrict__ x, const double *__restrict__ y,
-                              const double *__restrict__ z, Grid g, int32_t *__restrict__ cell_of,
-                              int32_t *__restrict__ cell_count)
+                              const double *__restrict__ z, const __grid_constant__ Grid g, GridSet set,
+                              int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count)
 {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    int cx = cell_coord(x[i], g.lo[0], g.w[0], g.dims[0]);
-    int cy = cell_coord(y[i], g.lo[1], g.w[1], g.dims[1]);
-    int cz = cell_coord(z[i], g.lo[2], g.w[2], g.dims[2]);
-    int c = (cz * g.dims[1] + cy) * g.dims[0] + cx;
+    const int sys = system_of(set.sys_off, set.nsys, i);
+    const Grid &G = set.nsys > 1 ? set.grids[sys] : g;
+    int cx = cell_coord(x[i], G.lo[0], G.w[0], G.dims[0]);
+    int cy = cell_coord(y[i], G.lo[1], G.w[1], G.dims[1]);
+    int cz = cell_coord(z[i], G.lo[2], G.w[2], G.dims[2]);
+    int c = (int)(set.nsys > 1 ? set.cell_off[sys] : 0) + (cz * G.dims[1] + cy) * G.dims[0] + cx;
     cell_of[i] = c;
     atomicAdd(cell_count + c, 1);
 }
@@ -521,23 +534,7 @@ __global__ void k_cell_scatter(int64_t n, const int32_t *__restrict__ cell_of, c
     sorted[start[c] + slot] = (int32_t)i;
 }
 
-// Order each cell's members by original index (insertion sort; cells hold tens of particles),
-// then gather positions (and the adjoint direction) into sorted order.
-__global__ void k_cell_order(int64_t ncells, const int32_t *__restrict__ start, int32_t *__restrict__ sorted)
-{
-    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncells) return;
-    int32_t b = start[c], e = start[c + 1];
-    for (int32_t p = b + 1; p < e; ++p) {
-        int32_t v = sorted[p], q = p - 1;
-        while (q >= b && sorted[q] > v) {
-            sorted[q + 1] = sorted[q];
-            --q;
-        }
-        sorted[q + 1] = v;
-    }
-}
-
+// Positions (and the adjoint direction) in sorted order.
 __global__ void k_gather(int64_t n, const int32_t *__restrict__ sorted, Pos pos, double *xs, double *ys, double *zs,
                          double *dxs, double *dys, double *dzs)
 {
@@ -554,21 +551,21 @@ __global__ void k_gather(int64_t n, const int32_t *__restrict__ sorted, Pos pos,
     }
 }
 
-cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, CellBufs &cb, bool with_dir, cudaStream_t st,
-                              int *launches)
+// Counting sort by cell.  The order inside a cell is the order of the scatter's atomics; nothing
+// depends on it (counts are order-independent, forces are accumulated with atomics anyway).
+cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, const GridSet &set, CellBufs &cb, bool with_dir,
+                              cudaStream_t st, int *launches)
 {
     const unsigned nb = (unsigned)((n + 255) / 256);
-    const unsigned cb_blocks = (unsigned)((g.ncells + 255) / 256);
     cudaError_t e;
     if ((e = cudaMemsetAsync(cb.cell_count, 0, sizeof(int32_t) * g.ncells, st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(cb.cell_fill, 0, sizeof(int32_t) * g.ncells, st)) != cudaSuccess) return e;
-    k_cell_assign<<<nb, 256, 0, st>>>(n, pos.x, pos.y, pos.z, g, cb.cell_of, cb.cell_count);
+    k_cell_assign<<<nb, 256, 0, st>>>(n, pos.x, pos.y, pos.z, g, set, cb.cell_of, cb.cell_count);
     k_cell_scan<<<1, 1024, 0, st>>>(g.ncells, cb.cell_count, cb.cell_start);
     k_cell_scatter<<<nb, 256, 0, st>>>(n, cb.cell_of, cb.cell_start, cb.cell_fill, cb.sorted);
-    k_cell_order<<<cb_blocks, 256, 0, st>>>(g.ncells, cb.cell_start, cb.sorted);
     k_gather<<<nb, 256, 0, st>>>(n, cb.sorted, pos, cb.xs, cb.ys, cb.zs, with_dir ? cb.dxs : nullptr,
                                  with_dir ? cb.dys : nullptr, with_dir ? cb.dzs : nullptr);
-    if (launches) *launches += 5;
+    if (launches) *launches += 4;
     return cudaGetLastError();
 }
 
@@ -586,7 +583,8 @@ cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, CellBufs &cb, b
 // and recompute.
 constexpr int NB_THREADS = 128;
 
-__global__ void __launch_bounds__(NB_THREADS) k_neighbors(Grid g, const double *__restrict__ xs,
+__global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant__ Grid g, GridSet set,
+                                                          const double *__restrict__ xs,
                                                           const double *__restrict__ ys,
                                                           const double *__restrict__ zs,
                                                           const int32_t *__restrict__ cell_start, int32_t *nbr,
@@ -605,17 +603,20 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(Grid g, const double *
     for (int64_t c = blockIdx.x; c < g.ncells; c += gridDim.x) {
         const int b0 = cell_start[c], e0 = cell_start[c + 1];
         if (b0 == e0) continue;
+        const int sys = system_of(set.cell_off, set.nsys, c);
+        const Grid &G = set.nsys > 1 ? set.grids[sys] : g;
         if (threadIdx.x == 0) {
-            const int cx = (int)(c % g.dims[0]), cy = (int)((c / g.dims[0]) % g.dims[1]),
-                      cz = (int)(c / ((int64_t)g.dims[0] * g.dims[1]));
+            const int64_t c0 = set.nsys > 1 ? set.cell_off[sys] : 0, lc = c - c0;
+            const int cx = (int)(lc % G.dims[0]), cy = (int)((lc / G.dims[0]) % G.dims[1]),
+                      cz = (int)(lc / ((int64_t)G.dims[0] * G.dims[1]));
             int ids[27], K = 0;
-            for (int oz = (g.dims[2] == 1 ? 0 : -1); oz <= (g.dims[2] == 1 ? 0 : 1); ++oz)
-                for (int oy = (g.dims[1] == 1 ? 0 : -1); oy <= (g.dims[1] == 1 ? 0 : 1); ++oy)
-                    for (int ox = (g.dims[0] == 1 ? 0 : -1); ox <= (g.dims[0] == 1 ? 0 : 1); ++ox) {
-                        const int nx = (cx + ox + g.dims[0]) % g.dims[0];
-                        const int ny = (cy + oy + g.dims[1]) % g.dims[1];
-                        const int nz = (cz + oz + g.dims[2]) % g.dims[2];
-                        const int nc = (nz * g.dims[1] + ny) * g.dims[0] + nx;
+            for (int oz = (G.dims[2] == 1 ? 0 : -1); oz <= (G.dims[2] == 1 ? 0 : 1); ++oz)
+                for (int oy = (G.dims[1] == 1 ? 0 : -1); oy <= (G.dims[1] == 1 ? 0 : 1); ++oy)
+                    for (int ox = (G.dims[0] == 1 ? 0 : -1); ox <= (G.dims[0] == 1 ? 0 : 1); ++ox) {
+                        const int nx = (cx + ox + G.dims[0]) % G.dims[0];
+                        const int ny = (cy + oy + G.dims[1]) % G.dims[1];
+                        const int nz = (cz + oz + G.dims[2]) % G.dims[2];
+                        const int nc = (int)c0 + (nz * G.dims[1] + ny) * G.dims[0] + nx;
                         if (nc < c) continue;
                         int q = K++;  // insertion by id (ids are distinct)
                         while (q > 0 && ids[q - 1] > nc) {
@@ -672,7 +673,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(Grid g, const double *
                         y = ys[t];
                         z = zs[t];
                     }
-                    pass = sqdist_periodic(xa, ya, za, x, y, z, g) <= g.sqcut;
+                    pass = sqdist_periodic(xa, ya, za, x, y, z, G) <= G.sqcut;
                 }
                 const unsigned m = __ballot_sync(0xffffffffu, pass);
                 const int off = cnt + __popc(m & ((1u << lane) - 1u));
@@ -690,7 +691,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(Grid g, const double *
 
 // Staging capacity: 2.5 times the expected candidate count (14 of the 27 cells have id >= c on
 // average), at least 256, at most 4096 (112 KiB).
-static int neighbor_stage_cap(const Grid &g, int64_t n)
+int neighbor_stage_cap(const Grid &g, int64_t n)
 {
     const double mean = (double)n / (double)g.ncells;
     const int cells = (g.dims[0] == 1 ? 1 : 3) * (g.dims[1] == 1 ? 1 : 3) * (g.dims[2] == 1 ? 1 : 3);
@@ -699,12 +700,13 @@ static int neighbor_stage_cap(const Grid &g, int64_t n)
     return want < 256 ? 256 : (want > 4096 ? 4096 : want);
 }
 
-cudaError_t launch_neighbors(int64_t n, const Grid &g, CellBufs &cb, cudaStream_t st)
+cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, int max_stage, CellBufs &cb,
+                             cudaStream_t st)
 {
-    const int max_stage = neighbor_stage_cap(g, n);
+    (void)n;
     const size_t smem = (size_t)max_stage * (3 * sizeof(double) + sizeof(int32_t));
     int64_t blocks = g.ncells < 65535 * 16 ? g.ncells : 65535 * 16;
-    k_neighbors<<<(unsigned)blocks, NB_THREADS, smem, st>>>(g, cb.xs, cb.ys, cb.zs, cb.cell_start, cb.nbr,
+    k_neighbors<<<(unsigned)blocks, NB_THREADS, smem, st>>>(g, set, cb.xs, cb.ys, cb.zs, cb.cell_start, cb.nbr,
                                                             cb.nbr_count, cb.max_count, cb.cap, max_stage);
     return cudaGetLastError();
 }
@@ -774,6 +776,7 @@ template <class S>
 __device__ __forceinline__ bool cut_inside(const P3Warp<S> &W, const CellBufs &cb, const Grid &g, int a, int b,
                                            V3<S> w, S cww, bool rawok, float band, float Lx, float Ly, float Lz)
 {
+    // g is the system's grid (L and cutoff of the exact test)
     if (SlotLayout<S>::mixed) {
         float d2;
         if (rawok) {
@@ -793,8 +796,8 @@ __device__ __forceinline__ bool cut_inside(const P3Warp<S> &W, const CellBufs &c
 }
 
 template <class S, bool ENERGY>
-__global__ void k_p3bca(int64_t n, Grid g, CellBufs cb, double nu_d, double *energy_out,
-                        unsigned long long *count_out, unsigned int *counter, float band, int raw_ok)
+__global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, CellBufs cb, double nu_d,
+                        double *energy_out, unsigned long long *count_out, unsigned int *counter)
 {
     using Acc = typename Traits<S>::Acc;
     using L = SlotLayout<S>;
@@ -818,10 +821,21 @@ __global__ void k_p3bca(int64_t n, Grid g, CellBufs cb, double nu_d, double *ene
     const S nu = constant<S>(nu_d), nu3 = constant<S>(-3.0 * nu_d), nu15 = constant<S>(15.0 * nu_d);
     const Out outs = {cb.fs[0], cb.fs[1], cb.fs[2], cb.hs[0], cb.hs[1], cb.hs[2]};
     const bool dual = Traits<S>::dual;
-    const float Lx = (float)g.L[0], Ly = (float)g.L[1], Lz = (float)g.L[2];
     const double cwrap = sqrt(g.sqcut) * 1.0000001;
     unsigned int cnt = 0;
     Acc en_acc = to_acc(szero<S>());
+    int cur_sys = 0;
+    // per-system count and energy, flushed when this warp moves on to another system
+    auto flush = [&](int sys) {
+        unsigned long long c64 = warp_sum_u64((unsigned long long)cnt);
+        if (lane == 0 && count_out && c64) atomicAdd(count_out + sys, c64);
+        cnt = 0;
+        if (ENERGY) {
+            Acc e = warp_sum(en_acc);
+            if (lane == 0) atomicAdd(energy_out + sys, acc_value(e));
+            en_acc = to_acc(szero<S>());
+        }
+    };
 
     unsigned int w = 0;
     if (lane == 0) w = atomicAdd(counter, 1u);
@@ -830,6 +844,15 @@ __global__ void k_p3bca(int64_t n, Grid g, CellBufs cb, double nu_d, double *ene
         unsigned int wn = 0;
         if (lane == 0) wn = atomicAdd(counter, 1u);
         const int s = (int)w;
+        const int sys = system_of(set.sys_off, set.nsys, s);
+        if (sys != cur_sys) {
+            flush(cur_sys);
+            cur_sys = sys;
+        }
+        const Grid &G = set.nsys > 1 ? set.grids[sys] : g;
+        const float Lx = (float)G.L[0], Ly = (float)G.L[1], Lz = (float)G.L[2];
+        const float band = G.band;
+        const int raw_ok = G.raw_ok;
         const int M = min(cb.nbr_count[s], cap);
         const double xi = cb.xs[s], yi = cb.ys[s], zi = cb.zs[s];
         const double dxi = dual ? cb.dxs[s] : 0.0, dyi = dual ? cb.dys[s] : 0.0, dzi = dual ? cb.dzs[s] : 0.0;
@@ -885,7 +908,7 @@ __global__ void k_p3bca(int64_t n, Grid g, CellBufs cb, double nu_d, double *ene
                 const V3<S> wv = third_edge(u, ul, v, vl);
                 const S cww = dot3(wv, wv);
                 bool inside = false;
-                if (act) inside = cut_inside(W, cb, g, a, b, wv, cww, rawok, band, Lx, Ly, Lz);
+                if (act) inside = cut_inside(W, cb, G, a, b, wv, cww, rawok, band, Lx, Ly, Lz);
                 cnt += inside ? 1u : 0u;
                 const ATCoef<S> cf =
                     at_coef<ENERGY>(aa, pd.w, cww, dot3(u, v), dot3(u, wv), dot3(v, wv), nu, nu3, nu15, inside, en);
@@ -960,13 +983,10 @@ __global__ void k_p3bca(int64_t n, Grid g, CellBufs cb, double nu_d, double *ene
         __syncwarp();
         w = __shfl_sync(0xffffffffu, wn, 0);
     }
-    unsigned long long c64 = warp_sum_u64((unsigned long long)cnt);
-    if (lane == 0 && count_out) atomicAdd(count_out, c64);
-    if (ENERGY) {
-        en_acc = warp_sum(en_acc);
-        if (lane == 0) atomicAdd(energy_out, acc_value(en_acc));
-    }
+    flush(cur_sys);
 }
+
+void fill_grid_test_params(Grid &g);
 
 // Half-width of the FP32 uncertainty band around cutoff^2 of the mixed test.  Each FP32 component
 // of the third edge (two-float difference of edges from i, then L - |d|) is within
@@ -988,6 +1008,12 @@ static int raw_test_ok(const Grid &g)
 {
     const double c = sqrt(g.sqcut) * 1.0000001;
     return (g.L[0] >= 4.0 * c && g.L[1] >= 4.0 * c && g.L[2] >= 4.0 * c) ? 1 : 0;
+}
+
+void fill_grid_test_params(Grid &g)
+{
+    g.band = guard_band(g);
+    g.raw_ok = raw_test_ok(g);
 }
 
 template <class S>
@@ -1030,30 +1056,29 @@ cudaError_t plan_p3bca(bool mixed, bool dual, bool energy, int cap, int warps, P
 }
 
 template <class S>
-static cudaError_t launch_p3bca_t(bool energy, int64_t n, const Grid &g, CellBufs &cb, double nu, double *eo,
-                                  unsigned long long *co, const P3Plan &plan, cudaStream_t st)
+static cudaError_t launch_p3bca_t(bool energy, int64_t n, const Grid &g, const GridSet &set, CellBufs &cb, double nu,
+                                  double *eo, unsigned long long *co, const P3Plan &plan, cudaStream_t st)
 {
     cudaError_t e;
     if ((e = cudaMemsetAsync(cb.work_counter, 0, sizeof(unsigned int), st)) != cudaSuccess) return e;
     if (energy)
-        k_p3bca<S, true><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, cb, nu, eo, co, cb.work_counter,
-                                                                         guard_band(g), raw_test_ok(g));
+        k_p3bca<S, true><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, set, cb, nu, eo, co, cb.work_counter);
     else
-        k_p3bca<S, false><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, cb, nu, eo, co, cb.work_counter,
-                                                                          guard_band(g), raw_test_ok(g));
+        k_p3bca<S, false><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, set, cb, nu, eo, co, cb.work_counter);
     return cudaGetLastError();
 }
 
-cudaError_t launch_p3bca(bool mixed, bool dual, bool energy, int64_t n, const Grid &g, CellBufs &cb, double nu,
-                         double *eo, unsigned long long *co, const P3Plan &plan, cudaStream_t st)
+cudaError_t launch_p3bca(bool mixed, bool dual, bool energy, int64_t n, const Grid &g, const GridSet &set,
+                         CellBufs &cb, double nu, double *eo, unsigned long long *co, const P3Plan &plan,
+                         cudaStream_t st)
 {
     if (n <= 0) return cudaSuccess;
     if (dual) {
-        if (mixed) return launch_p3bca_t<Dual<float>>(energy, n, g, cb, nu, eo, co, plan, st);
-        return launch_p3bca_t<Dual<double>>(energy, n, g, cb, nu, eo, co, plan, st);
+        if (mixed) return launch_p3bca_t<Dual<float>>(energy, n, g, set, cb, nu, eo, co, plan, st);
+        return launch_p3bca_t<Dual<double>>(energy, n, g, set, cb, nu, eo, co, plan, st);
     }
-    if (mixed) return launch_p3bca_t<float>(energy, n, g, cb, nu, eo, co, plan, st);
-    return launch_p3bca_t<double>(energy, n, g, cb, nu, eo, co, plan, st);
+    if (mixed) return launch_p3bca_t<float>(energy, n, g, set, cb, nu, eo, co, plan, st);
+    return launch_p3bca_t<double>(energy, n, g, set, cb, nu, eo, co, plan, st);
 }
 
 __global__ void k_unsort(int64_t n, const int32_t *__restrict__ sorted, const double *__restrict__ f0,
