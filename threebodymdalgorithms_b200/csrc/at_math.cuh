@@ -80,11 +80,20 @@ struct ATCoef {
 // gives exact zeros (masked lanes, k <= j, padding) without anything inf or NaN reaching the
 // result.  nu3 = -3 nu, nu15 = 15 nu.  Returns m = -3 nu t^5 and B2 = m + 15 nu t^5 D t^2; ENERGY
 // adds the triplet energy nu t^3 (1 - 3 D t^2) to `e`.
+// One Newton step for x^(-1/2): t (1.5 - 0.5 x t^2).  Used for FP32 when the energy is also wanted:
+// the energy sum of a small system can cancel, so its terms get the refined value.
+__device__ __forceinline__ float refine_rsqrt(float x, float t) { return t * fmaf(-0.5f * x, t * t, 1.5f); }
+__device__ __forceinline__ double refine_rsqrt(double, double t) { return t; }
+template <class T>
+__device__ __forceinline__ Dual<T> refine_rsqrt(Dual<T>, Dual<T> t) { return t; }
+
 template <bool ENERGY, class S>
 __device__ __forceinline__ void at_core(S a, S b, S c, S p, S q, S s, S nu, S nu3, S nu15, bool valid, S &e, S &m,
                                         S &B2)
 {
-    S t = rsqrt_(a * b * c);
+    const S x = a * b * c;
+    S t = rsqrt_(x);
+    if (ENERGY) t = refine_rsqrt(x, t);
     if (!valid) t = zero_like(t);
     S t2 = t * t;
     S t5 = t2 * t2 * t;

@@ -86,6 +86,9 @@ struct tbmd_ctx {
     Grid grid{};          // single system, or for a batch: first system's grid with ncells = all cells
     GridSet gset{};       // device tables of the systems being evaluated
     DevBuf gset_single;   // Grid[1] + cell_off[2] + sys_off[2] of the single-system case
+    DevBuf ncell_tab;     // neighbour-cell table of the cells being evaluated (27 per cell)
+    Grid ncell_grid{};    // grid the single-system table was built for
+    bool ncell_single = false;
     int max_stage = 256;  // neighbour staging capacity
     DevBuf cell_n, cell_c, nbr_buf;
     int64_t cell_bufs_n = -1, cell_bufs_cells = -1;
@@ -355,6 +358,16 @@ static tbmd_status ensure_cells(tbmd_ctx *ctx, int64_t n, bool dual, bool energy
     ctx->gset = GridSet{(const Grid *)base, (const int64_t *)(base + offsetof(decltype(tab), cell_off)),
                         (const int64_t *)(base + offsetof(decltype(tab), sys_off)), 1};
     ctx->max_stage = neighbor_stage_cap(ctx->grid, n);
+    if (!ctx->ncell_single || std::memcmp(&ctx->ncell_grid, &ctx->grid, sizeof(Grid)) != 0) {
+        std::vector<int32_t> tab27((size_t)ctx->grid.ncells * 27);
+        neighbor_cell_table(ctx->grid, 0, tab27.data());
+        CK(ctx->ncell_tab.ensure(sizeof(int32_t) * tab27.size()));
+        CK(cudaMemcpyAsync(ctx->ncell_tab.p, tab27.data(), sizeof(int32_t) * tab27.size(), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        ctx->ncell_grid = ctx->grid;
+        ctx->ncell_single = true;
+    }
     return ensure_cell_bufs(ctx, n, ctx->grid.ncells, dual, energy);
 }
 
@@ -393,7 +406,7 @@ static tbmd_status enqueue_forces(tbmd_ctx *ctx, int64_t n, Pos pos, Out out, bo
         phase_mark(ctx, st, PH_CELLS, *nl);
         CK(launch_cell_build(n, pos, ctx->grid, ctx->gset, cb, dual, st, nl));
         phase_mark(ctx, st, PH_NEIGHBORS, *nl);
-        CK(launch_neighbors(n, ctx->grid, ctx->gset, ctx->max_stage, cb, st));
+        CK(launch_neighbors(n, ctx->grid, ctx->gset, ctx->ncell_tab.as<int32_t>(), ctx->max_stage, cb, st));
         *nl += 1;
         for (int k = 0; k < 3; ++k) {
             CK(cudaMemsetAsync(cb.fs[k], 0, sizeof(double) * n, st));
@@ -582,7 +595,7 @@ void tbmd_destroy(tbmd_ctx *ctx)
     for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
     for (DevBuf *b : {&ctx->state, &ctx->snapshot, &ctx->scalars, &ctx->step_counts, &ctx->prefix, &ctx->partial,
                       &ctx->cell_n, &ctx->cell_c, &ctx->nbr_buf, &ctx->dirs, &ctx->hvp, &ctx->gset_single,
-                      &ctx->sweep_sys, &ctx->bpos, &ctx->bout, &ctx->bsys, &ctx->bprefix})
+                      &ctx->sweep_sys, &ctx->bpos, &ctx->bout, &ctx->bsys, &ctx->bprefix, &ctx->ncell_tab})
         b->release();
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -1138,6 +1151,11 @@ static tbmd_status batch_eval(tbmd_ctx *ctx, int32_t nsys, const int64_t *offset
             const int sc = neighbor_stage_cap(grids[s], e - b);
             stage = sc > stage ? sc : stage;
         }
+        std::vector<int32_t> tab27((size_t)cell_off[nsys] * 27);
+        for (int s = 0; s < nsys; ++s) neighbor_cell_table(grids[s], cell_off[s], tab27.data());
+        CK(ctx->ncell_tab.ensure(sizeof(int32_t) * tab27.size()));
+        CK(cudaMemcpyAsync(ctx->ncell_tab.p, tab27.data(), sizeof(int32_t) * tab27.size(), cudaMemcpyHostToDevice, sm));
+        ctx->ncell_single = false;  // the single-system table is rebuilt on the next single evaluation
         const size_t gbytes = sizeof(Grid) * nsys, obytes = sizeof(int64_t) * (nsys + 1);
         CK(ctx->bsys.ensure(gbytes + 2 * obytes + 64));
         char *tb = ctx->bsys.as<char>();
@@ -1160,7 +1178,7 @@ static tbmd_status batch_eval(tbmd_ctx *ctx, int32_t nsys, const int64_t *offset
             CK(cudaMemsetAsync(E, 0, sizeof(double) * 2 * nsys, sm));
             CellBufs &cb = ctx->cb;
             CK(launch_cell_build(N, pos, ctx->grid, ctx->gset, cb, dual, sm, &nl));
-            CK(launch_neighbors(N, ctx->grid, ctx->gset, ctx->max_stage, cb, sm));
+            CK(launch_neighbors(N, ctx->grid, ctx->gset, ctx->ncell_tab.as<int32_t>(), ctx->max_stage, cb, sm));
             for (int k = 0; k < 3; ++k) {
                 CK(cudaMemsetAsync(cb.fs[k], 0, sizeof(double) * N, sm));
                 if (dual) CK(cudaMemsetAsync(cb.hs[k], 0, sizeof(double) * N, sm));

@@ -262,9 +262,11 @@ struct CellBufs {
 // For a GridSet, g is the first system's grid with ncells = total cells over all systems.
 cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, const GridSet &set, CellBufs &cb, bool with_dir,
                               cudaStream_t st, int *launches);
-cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, int max_stage, CellBufs &cb,
-                             cudaStream_t st);
+cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, const int32_t *nbr_cells, int max_stage,
+                             CellBufs &cb, cudaStream_t st);
 int neighbor_stage_cap(const Grid &g, int64_t n);
+// host: neighbour-cell table rows (27 ints per cell, ids >= the cell's own, ascending, -1 padded)
+void neighbor_cell_table(const Grid &g, int64_t cell0, int32_t *out);
 // Launch shape of the P3BCA triplet kernel for a list capacity; computed outside graph capture.
 struct P3Plan {
     int warps = 0;

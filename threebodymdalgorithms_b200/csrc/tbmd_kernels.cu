@@ -574,16 +574,18 @@ cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, const GridSet &
 //
 // Block per cell c.  Particles are counting-sorted by cell id, so the candidates t > s of a
 // particle s in c are: the particles of c after s, and all particles of the neighbour cells with
-// id > c.  The block lists the neighbour cells with id >= c in increasing id order and stages
-// their particles (positions and sorted indices) in shared memory in that order; the candidate
-// list of the i-th particle of c is then the suffix starting at i + 1.  Warps take the particles of
-// c in turn and sweep their suffix 32 candidates at a time, writing survivors compacted by ballot.
-// A cell whose candidates exceed the staging capacity reads them from global memory instead.
-// Lists longer than cap are truncated; the largest length is recorded so the host can enlarge cap
-// and recompute.
+// id > c.  nbr_cells (built on the host with the grid) lists, per cell, its neighbour cells with
+// id >= c in increasing id order (-1 padded to 27).  The block scans their sizes, stages their
+// particles (positions and sorted indices) in shared memory in that order - cell by cell, so every
+// copy is coalesced - and the candidates of the i-th particle of c are the suffix after i.  Warps
+// take the particles of c in turn and sweep their suffix 32 candidates at a time, writing survivors
+// compacted by ballot.  A cell whose candidates exceed the staging capacity reads them from global
+// memory instead.  Lists longer than cap are truncated; the largest length is recorded so the host
+// can enlarge cap and recompute.
 constexpr int NB_THREADS = 128;
 
 __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant__ Grid g, GridSet set,
+                                                          const int32_t *__restrict__ nbr_cells,
                                                           const double *__restrict__ xs,
                                                           const double *__restrict__ ys,
                                                           const double *__restrict__ zs,
@@ -596,8 +598,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
     double *sy = sx + max_stage;
     double *sz = sy + max_stage;
     int32_t *st = (int32_t *)(sz + max_stage);
-    __shared__ int cstart[27], cpre[28];
-    __shared__ int nk;
+    __shared__ int cstart[32], cpre[33];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int NW = NB_THREADS / 32;
     for (int64_t c = blockIdx.x; c < g.ncells; c += gridDim.x) {
@@ -605,53 +606,40 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
         if (b0 == e0) continue;
         const int sys = system_of(set.cell_off, set.nsys, c);
         const Grid &G = set.nsys > 1 ? set.grids[sys] : g;
-        if (threadIdx.x == 0) {
-            const int64_t c0 = set.nsys > 1 ? set.cell_off[sys] : 0, lc = c - c0;
-            const int cx = (int)(lc % G.dims[0]), cy = (int)((lc / G.dims[0]) % G.dims[1]),
-                      cz = (int)(lc / ((int64_t)G.dims[0] * G.dims[1]));
-            int ids[27], K = 0;
-            for (int oz = (G.dims[2] == 1 ? 0 : -1); oz <= (G.dims[2] == 1 ? 0 : 1); ++oz)
-                for (int oy = (G.dims[1] == 1 ? 0 : -1); oy <= (G.dims[1] == 1 ? 0 : 1); ++oy)
-                    for (int ox = (G.dims[0] == 1 ? 0 : -1); ox <= (G.dims[0] == 1 ? 0 : 1); ++ox) {
-                        const int nx = (cx + ox + G.dims[0]) % G.dims[0];
-                        const int ny = (cy + oy + G.dims[1]) % G.dims[1];
-                        const int nz = (cz + oz + G.dims[2]) % G.dims[2];
-                        const int nc = (int)c0 + (nz * G.dims[1] + ny) * G.dims[0] + nx;
-                        if (nc < c) continue;
-                        int q = K++;  // insertion by id (ids are distinct)
-                        while (q > 0 && ids[q - 1] > nc) {
-                            ids[q] = ids[q - 1];
-                            --q;
-                        }
-                        ids[q] = nc;
-                    }
-            int run = 0;
-            for (int k = 0; k < K; ++k) {
-                cstart[k] = cell_start[ids[k]];
-                cpre[k] = run;
-                run += cell_start[ids[k] + 1] - cstart[k];
+        if (warp == 0) {
+            const int nc = lane < 27 ? nbr_cells[c * 27 + lane] : -1;
+            const int cs = nc >= 0 ? cell_start[nc] : 0;
+            const int len = nc >= 0 ? cell_start[nc + 1] - cs : 0;
+            int incl = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
             }
-            cpre[K] = run;
-            nk = K;
+            cstart[lane] = cs;
+            cpre[lane] = incl - len;
+            if (lane == 31) cpre[32] = incl;
         }
         __syncthreads();
-        const int K = nk, T = cpre[K];
+        const int T = cpre[32];
         const bool staged = T <= max_stage;
         if (staged) {
-            for (int q = threadIdx.x; q < T; q += NB_THREADS) {
-                int k = 0;
-                while (k + 1 < K && cpre[k + 1] <= q) ++k;
-                const int t = cstart[k] + (q - cpre[k]);
-                sx[q] = xs[t];
-                sy[q] = ys[t];
-                sz[q] = zs[t];
-                st[q] = t;
+            for (int k = 0; k < 27; ++k) {
+                const int beg = cpre[k], len = cpre[k + 1] - beg;
+                if (len == 0) continue;
+                for (int i = threadIdx.x; i < len; i += NB_THREADS) {
+                    const int t = cstart[k] + i;
+                    sx[beg + i] = xs[t];
+                    sy[beg + i] = ys[t];
+                    sz[beg + i] = zs[t];
+                    st[beg + i] = t;
+                }
             }
         }
         __syncthreads();
         for (int sl = warp; sl < e0 - b0; sl += NW) {
             const int s = b0 + sl;  // cell c comes first in the candidate order: q = sl
-            const double xa = xs[s], ya = ys[s], za = zs[s];
+            const double xa = staged ? sx[sl] : xs[s], ya = staged ? sy[sl] : ys[s], za = staged ? sz[sl] : zs[s];
             int cnt = 0;
             int32_t *dst = nbr + (int64_t)s * cap;
             for (int q0 = sl + 1; q0 < T; q0 += 32) {
@@ -667,7 +655,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
                         z = sz[q];
                     } else {
                         int k = 0;
-                        while (k + 1 < K && cpre[k + 1] <= q) ++k;
+                        while (k < 26 && cpre[k + 1] <= q) ++k;
                         t = cstart[k] + (q - cpre[k]);
                         x = xs[t];
                         y = ys[t];
@@ -700,14 +688,44 @@ int neighbor_stage_cap(const Grid &g, int64_t n)
     return want < 256 ? 256 : (want > 4096 ? 4096 : want);
 }
 
-cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, int max_stage, CellBufs &cb,
-                             cudaStream_t st)
+// Per cell of grid g (cells numbered from cell0), its neighbour cells with id >= its own id in
+// increasing order, -1 padded to 27 entries.
+void neighbor_cell_table(const Grid &g, int64_t cell0, int32_t *out)
+{
+    const int ox = g.dims[0] == 1 ? 0 : 1, oy = g.dims[1] == 1 ? 0 : 1, oz = g.dims[2] == 1 ? 0 : 1;
+    for (int64_t lc = 0; lc < g.ncells; ++lc) {
+        const int cx = (int)(lc % g.dims[0]), cy = (int)((lc / g.dims[0]) % g.dims[1]),
+                  cz = (int)(lc / ((int64_t)g.dims[0] * g.dims[1]));
+        int32_t ids[27];
+        int K = 0;
+        for (int dz = -oz; dz <= oz; ++dz)
+            for (int dy = -oy; dy <= oy; ++dy)
+                for (int dx = -ox; dx <= ox; ++dx) {
+                    const int nx = (cx + dx + g.dims[0]) % g.dims[0];
+                    const int ny = (cy + dy + g.dims[1]) % g.dims[1];
+                    const int nz = (cz + dz + g.dims[2]) % g.dims[2];
+                    const int64_t nc = (int64_t)(nz * g.dims[1] + ny) * g.dims[0] + nx;
+                    if (nc < lc) continue;
+                    int q = K++;
+                    while (q > 0 && ids[q - 1] > nc + cell0) {
+                        ids[q] = ids[q - 1];
+                        --q;
+                    }
+                    ids[q] = (int32_t)(nc + cell0);
+                }
+        int32_t *row = out + (cell0 + lc) * 27;
+        for (int k = 0; k < 27; ++k) row[k] = k < K ? ids[k] : -1;
+    }
+}
+
+cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, const int32_t *nbr_cells, int max_stage,
+                             CellBufs &cb, cudaStream_t st)
 {
     (void)n;
     const size_t smem = (size_t)max_stage * (3 * sizeof(double) + sizeof(int32_t));
     int64_t blocks = g.ncells < 65535 * 16 ? g.ncells : 65535 * 16;
-    k_neighbors<<<(unsigned)blocks, NB_THREADS, smem, st>>>(g, set, cb.xs, cb.ys, cb.zs, cb.cell_start, cb.nbr,
-                                                            cb.nbr_count, cb.max_count, cb.cap, max_stage);
+    k_neighbors<<<(unsigned)blocks, NB_THREADS, smem, st>>>(g, set, nbr_cells, cb.xs, cb.ys, cb.zs, cb.cell_start,
+                                                            cb.nbr, cb.nbr_count, cb.max_count, cb.cap, max_stage);
     return cudaGetLastError();
 }
 
@@ -772,9 +790,11 @@ struct P3Warp {
 };
 
 // Third-edge cutoff decision for slots a (own) and b (partner) with third edge w.
+// sq_lo / sq_hi: cutoff^2 minus / plus the FP32 band, hoisted out of the pair loop by the caller.
 template <class S>
 __device__ __forceinline__ bool cut_inside(const P3Warp<S> &W, const CellBufs &cb, const Grid &g, int a, int b,
-                                           V3<S> w, S cww, bool rawok, float band, float Lx, float Ly, float Lz)
+                                           V3<S> w, S cww, bool rawok, float sq_lo, float sq_hi, float Lx, float Ly,
+                                           float Lz)
 {
     // g is the system's grid (L and cutoff of the exact test)
     if (SlotLayout<S>::mixed) {
@@ -786,9 +806,8 @@ __device__ __forceinline__ bool cut_inside(const P3Warp<S> &W, const CellBufs &c
             const float mx = fminf(ax, Lx - ax), my = fminf(ay, Ly - ay), mz = fminf(az, Lz - az);
             d2 = fmaf(mx, mx, fmaf(my, my, mz * mz));
         }
-        const float sq = (float)g.sqcut;
-        if (d2 <= sq - band) return true;
-        if (d2 > sq + band) return false;
+        if (d2 <= sq_lo) return true;
+        if (d2 > sq_hi) return false;
         const int32_t ta = W.idx[a], tb = W.idx[b];
         return sqdist_periodic(cb.xs[ta], cb.ys[ta], cb.zs[ta], cb.xs[tb], cb.ys[tb], cb.zs[tb], g) <= g.sqcut;
     }
@@ -851,7 +870,7 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
         }
         const Grid &G = set.nsys > 1 ? set.grids[sys] : g;
         const float Lx = (float)G.L[0], Ly = (float)G.L[1], Lz = (float)G.L[2];
-        const float band = G.band;
+        const float sq_lo = (float)G.sqcut - G.band, sq_hi = (float)G.sqcut + G.band;
         const int raw_ok = G.raw_ok;
         const int M = min(cb.nbr_count[s], cap);
         const double xi = cb.xs[s], yi = cb.ys[s], zi = cb.zs[s];
@@ -908,7 +927,7 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
                 const V3<S> wv = third_edge(u, ul, v, vl);
                 const S cww = dot3(wv, wv);
                 bool inside = false;
-                if (act) inside = cut_inside(W, cb, G, a, b, wv, cww, rawok, band, Lx, Ly, Lz);
+                if (act) inside = cut_inside(W, cb, G, a, b, wv, cww, rawok, sq_lo, sq_hi, Lx, Ly, Lz);
                 cnt += inside ? 1u : 0u;
                 const ATCoef<S> cf =
                     at_coef<ENERGY>(aa, pd.w, cww, dot3(u, v), dot3(u, wv), dot3(v, wv), nu, nu3, nu15, inside, en);
