@@ -80,6 +80,11 @@ class ClockSampler:
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the first sample arrives after nvidia-smi has started; wait for it (at most 5 s) so
+            # that the samples cover the timed region
+            t0 = time.monotonic()
+            while not self.lines and time.monotonic() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.02)
         except OSError:
             self.proc = None
         return self
@@ -200,7 +205,7 @@ def run_ours(args, world, rank, local):
         return c
 
     result = {}
-    for prec in ([args.precision] + (["fp64"] if args.precision != "fp64" else [])):
+    for prec in ([args.precision] + (["fp64"] if args.precision != "fp64" and not args.no_fp64 else [])):
         ctx = new_ctx(prec)
         reset = (lambda c=ctx: c.set_state(st))
         if args.autotune:
@@ -421,7 +426,7 @@ WORKLOAD_TRIPLETS = {"c1": math.comb(512, 3), "c2": math.comb(8192, 3), "c3": 48
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="c3")
@@ -429,6 +434,7 @@ def main():
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 run beside the mixed one")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
