@@ -168,20 +168,22 @@ def timed_steps(ctx, steps, flush, torch, reset=None):
     workload's input state is restored, so every step is the same step of the same input, and L2
     is flushed."""
     stream = torch.cuda.current_stream()
-    times, counts = [], []
+    times, counts, launches = [], [], 0
     for _ in range(steps):
         if reset is not None:
             reset()
         flush.fill_(1.0)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        l0 = ctx.kernel_launches()
         e0.record(stream)
         c = ctx.step(1)
         e1.record(stream)
+        launches += ctx.kernel_launches() - l0
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
         counts.append(int(c[0]))
-    return times, counts
+    return times, counts, launches
 
 
 def run_ours(args, world, rank, local):
@@ -212,10 +214,8 @@ def run_ours(args, world, rank, local):
             ctx.autotune(str(ROOT / "profiles" / "autotune_cache.jsonl"))
         timed_steps(ctx, args.warmup, flush, torch, reset)
         barrier(world)
-        l0 = ctx.kernel_launches()
         with ClockSampler(local) as clk:
-            times, counts = timed_steps(ctx, args.steps, flush, torch, reset)
-        launches = ctx.kernel_launches() - l0
+            times, counts, launches = timed_steps(ctx, args.steps, flush, torch, reset)
         barrier(world)
         total_ms = allreduce_max(sum(times), world)
         result[prec] = dict(times=times, counts=counts, total_ms=total_ms, launches=launches, clocks=clk.summary(),

@@ -372,8 +372,11 @@ uint64_t tbo_forces_cells(int64_t n, const double *x, const double *y, const dou
 
 /* Triplet energy from dot products: u = xj - xi, v = xk - xi, w = xk - xj,
  * cos_i cos_j cos_k = -(u.v)(u.w)(v.w) / (|u|^2 |v|^2 |w|^2). */
-static inline double at_energy(double nu, const double *x, const double *y, const double *z, int64_t i, int64_t j,
-                               int64_t k)
+/* scale = 0: the triplet energy nu (1 + 3 cos cos cos) / (r1 r2 r3)^3.
+ * scale = 1: its magnitude scale |nu| (1 + 3 |cos cos cos|) / (r1 r2 r3)^3, the size of both parts of
+ * the term, against which a rounding error in the geometry is measured. */
+static inline double at_energy_s(double nu, const double *x, const double *y, const double *z, int64_t i,
+                                 int64_t j, int64_t k, int scale)
 {
     double ux = x[j] - x[i], uy = y[j] - y[i], uz = z[j] - z[i];
     double vx = x[k] - x[i], vy = y[k] - y[i], vz = z[k] - z[i];
@@ -382,12 +385,21 @@ static inline double at_energy(double nu, const double *x, const double *y, cons
     double uv = ux * vx + uy * vy + uz * vz, uw = ux * wx + uy * wy + uz * wz, vw = vx * wx + vy * wy + vz * wz;
     double cosprod = -(uv * uw * vw) / (uu * vv * ww);
     double r3 = sqrt(uu * vv * ww);
+    if (scale) return fabs(nu) * (1.0 + 3.0 * fabs(cosprod)) / (r3 * r3 * r3);
     return nu * (1.0 + 3.0 * cosprod) / (r3 * r3 * r3);
+}
+static inline double at_energy(double nu, const double *x, const double *y, const double *z, int64_t i, int64_t j,
+                               int64_t k)
+{
+    return at_energy_s(nu, x, y, z, i, j, k, 0);
 }
 
 /* Total AT energy over the triplet set of tbo_forces_* (cells used when cutoff > 0). */
-double tbo_energy(int64_t n, const double *x, const double *y, const double *z, double nu, double cutoff,
-                  const double *L, const double *lo, int nthreads)
+/* Sum over the triplet set of E_t (absval = 0) or of the magnitude scales of at_energy_s (absval =
+ * 1).  The second is the scale of the energy's rounding error: the terms have both signs
+ * (1 + 3 cos cos cos < 0 for nearly collinear triplets), so |sum E_t| can be much smaller. */
+static double energy_sum(int64_t n, const double *x, const double *y, const double *z, double nu, double cutoff,
+                         const double *L, const double *lo, int nthreads, int absval)
 {
     nthreads = clamp_threads(nthreads);
     double e = 0.0;
@@ -403,7 +415,7 @@ double tbo_energy(int64_t n, const double *x, const double *y, const double *z, 
                 for (int64_t q = p + 1; q < len; ++q) {
                     int64_t j = l[p], k = l[q];
                     if (sqdist_periodic(x[j], y[j], z[j], x[k], y[k], z[k], L) > sq) continue;
-                    e += at_energy(nu, x, y, z, i, j, k);
+                    e += at_energy_s(nu, x, y, z, i, j, k, absval);
                 }
         }
         free(start);
@@ -412,9 +424,23 @@ double tbo_energy(int64_t n, const double *x, const double *y, const double *z, 
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads) reduction(+ : e)
         for (int64_t i = 0; i < n; ++i)
             for (int64_t j = i + 1; j < n; ++j)
-                for (int64_t k = j + 1; k < n; ++k) e += at_energy(nu, x, y, z, i, j, k);
+                for (int64_t k = j + 1; k < n; ++k) {
+                    e += at_energy_s(nu, x, y, z, i, j, k, absval);
+                }
     }
     return e;
+}
+
+double tbo_energy(int64_t n, const double *x, const double *y, const double *z, double nu, double cutoff,
+                  const double *L, const double *lo, int nthreads)
+{
+    return energy_sum(n, x, y, z, nu, cutoff, L, lo, nthreads, 0);
+}
+
+double tbo_energy_abs(int64_t n, const double *x, const double *y, const double *z, double nu, double cutoff,
+                      const double *L, const double *lo, int nthreads)
+{
+    return energy_sum(n, x, y, z, nu, cutoff, L, lo, nthreads, 1);
 }
 
 /* Particle::UpdatePredictorStage (structs.hpp:40-55): x += v*dt + (aX, aX, aX) * (dt*dt*0.5).

@@ -57,6 +57,8 @@ def lib():
                                          C.POINTER(C.c_int32)]
         _lib.tbo_energy.argtypes = [i64, d, d, d, C.c_double, C.c_double, d, d, C.c_int]
         _lib.tbo_energy.restype = C.c_double
+        _lib.tbo_energy_abs.argtypes = [i64, d, d, d, C.c_double, C.c_double, d, d, C.c_int]
+        _lib.tbo_energy_abs.restype = C.c_double
         _lib.tbo_predictor.argtypes = [i64, d, d, d, d, d, d, d, C.c_double]
         _lib.tbo_update.argtypes = [i64, d, d, d, d, d, d, d, d, d, d, C.c_double, d]
         _lib.tbo_simulate.argtypes = [C.c_int, C.c_int, i64] + [d] * 13 + [C.c_double, d, C.c_double,
@@ -131,6 +133,17 @@ def energy(x, y, z, nu=1.0, cutoff=-1.0, L=None, lo=None, nthreads=0):
         L, lo = domain(x, y, z)
     L, lo = _f64(L), _f64(lo)
     return float(lib().tbo_energy(len(x), _p(x), _p(y), _p(z), nu, cutoff, _p(L), _p(lo), nthreads))
+
+
+def energy_abs(x, y, z, nu=1.0, cutoff=-1.0, L=None, lo=None, nthreads=0):
+    """Sum over the same triplet set of |nu| (1 + 3 |cos cos cos|) / (r1 r2 r3)^3, the magnitude of
+    both parts of each term: the scale of the energy's rounding error (the terms have both signs,
+    and one term can cancel inside, so the energy itself can be much smaller)."""
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    if L is None or lo is None:
+        L, lo = domain(x, y, z)
+    L, lo = _f64(L), _f64(lo)
+    return float(lib().tbo_energy_abs(len(x), _p(x), _p(y), _p(z), nu, cutoff, _p(L), _p(lo), nthreads))
 
 
 FIELDS = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "fx", "fy", "fz")

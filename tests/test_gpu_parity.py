@@ -28,7 +28,11 @@ MIXED_FORCE_TOL = 1e-5
 MIXED_STATE_TOL = 1e-6
 MIXED_MULTISTEP_POS_TOL = 1e-4
 MIXED_MULTISTEP_TOL = 1e-2
-MIXED_ENERGY_TOL = 5e-6
+# Mixed energies: |E - E_ref| <= MIXED_ENERGY_TOL * S with S = sum over triplets of
+# |nu| (1 + 3 |cos cos cos|) / (r1 r2 r3)^3 (oracle energy_abs).  The triplet terms have both signs
+# and a term can cancel inside (1 + 3 cos cos cos), so |E| can be far smaller than S (by 37x in the
+# batched test systems); FP32 geometry rounds each part of a term to about 1e-6 of its size.
+MIXED_ENERGY_TOL = 2e-6
 STATE = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "fx", "fy", "fz")
 
 
@@ -119,6 +123,7 @@ def test_auta_vs_oracle_n1024():
     fx, fy, fz, c = O.forces(st["x"], st["y"], st["z"], 1.0, -1.0, nthreads=0)
     ref = np.stack([fx, fy, fz], 1)
     e_ref = O.energy(st["x"], st["y"], st["z"], 1.0, -1.0)
+    e_abs = O.energy_abs(st["x"], st["y"], st["z"], 1.0, -1.0)
     for algo in ("auta", "nata"):
         f64, e64, c64 = forces_of(algo, "fp64", st)
         fmx, emx, cmx = forces_of(algo, "mixed", st)
@@ -126,7 +131,7 @@ def test_auta_vs_oracle_n1024():
         assert rel_l2(f64, ref) <= FP64_TOL
         assert rel_l2(fmx, ref) <= MIXED_FORCE_TOL
         assert abs(e64 - e_ref) <= 1e-12 * abs(e_ref)
-        assert abs(emx - e_ref) <= MIXED_ENERGY_TOL * abs(e_ref)
+        assert abs(emx - e_ref) <= MIXED_ENERGY_TOL * e_abs
 
 
 def test_c2_n8192_nata_auta_fp64_mixed():
@@ -142,7 +147,9 @@ def test_c2_n8192_nata_auta_fp64_mixed():
     assert rel_l2(fm, fa) <= MIXED_FORCE_TOL
     assert rel_l2(fnm, fa) <= MIXED_FORCE_TOL
     assert np.abs(fa.sum(0)).max() <= 1e-9 * np.abs(fa).max() * 8192
-    assert abs(ea - en) <= 1e-12 * abs(ea) and abs(em - ea) <= MIXED_ENERGY_TOL * abs(ea)
+    # sum |E_t| over 9.2e10 triplets is too costly for the oracle here; for a uniform system it is
+    # within a few percent of |E|, so the bound is taken against |E| with a 5x margin
+    assert abs(ea - en) <= 1e-12 * abs(ea) and abs(em - ea) <= 5 * MIXED_ENERGY_TOL * abs(ea)
 
 
 @pytest.mark.parametrize("cutoff", [2.0, 1.5])
@@ -204,10 +211,11 @@ def test_energy_p3bca_vs_oracle():
     st = generators.uniform(n, (side, side, side))
     L, lo = O.domain(st["x"], st["y"], st["z"])
     e_ref = O.energy(st["x"], st["y"], st["z"], 1.0, 2.0, L, lo)
+    e_abs = O.energy_abs(st["x"], st["y"], st["z"], 1.0, 2.0, L, lo)
     _, e64, _ = forces_of("p3bca", "fp64", st, 2.0)
     _, emx, _ = forces_of("p3bca", "mixed", st, 2.0)
     assert abs(e64 - e_ref) <= 1e-12 * abs(e_ref)
-    assert abs(emx - e_ref) <= MIXED_ENERGY_TOL * abs(e_ref)
+    assert abs(emx - e_ref) <= MIXED_ENERGY_TOL * e_abs
 
 
 def test_clustered_capacity_retry():

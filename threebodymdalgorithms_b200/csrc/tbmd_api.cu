@@ -63,6 +63,7 @@ struct tbmd_ctx {
     DevBuf state;
     double *s[13] = {};
     DevBuf snapshot;  // copy of x..az taken before a multi-step run (capacity retry)
+    DevBuf staging;   // tbmd_set_particles: incoming arrays and their check result
 
     // scalars: energy, count_cur, step counter, per-step counts
     DevBuf scalars;
@@ -86,6 +87,7 @@ struct tbmd_ctx {
     Grid grid{};          // single system, or for a batch: first system's grid with ncells = all cells
     GridSet gset{};       // device tables of the systems being evaluated
     DevBuf gset_single;   // Grid[1] + cell_off[2] + sys_off[2] of the single-system case
+    alignas(8) unsigned char gset_host[256] = {};  // host copy of what gset_single holds
     DevBuf ncell_tab;     // neighbour-cell table of the cells being evaluated (27 per cell)
     Grid ncell_grid{};    // grid the single-system table was built for
     bool ncell_single = false;
@@ -96,6 +98,7 @@ struct tbmd_ctx {
     int cap = 0;
     int p3_warps = 4;
     P3Plan plan{};
+    int plan_key[5] = {-1, -1, -1, -1, -1};  // (mixed, dual, energy, cap, warps) the plan was made for
 
     // adjoint / device-variant scratch
     DevBuf dirs, hvp;
@@ -337,7 +340,11 @@ static tbmd_status ensure_cell_bufs(tbmd_ctx *ctx, int64_t n, int64_t nc, bool d
     ctx->cb.max_count = (int32_t *)(ctx->scalars.as<char>() + 28);
     ctx->cb.work_counter = (unsigned int *)(ctx->scalars.as<char>() + 32);
     ctx->cb.cap = ctx->cap;
-    CK(plan_p3bca(mixed(ctx), dual, energy, ctx->cap, ctx->p3_warps, &ctx->plan));
+    const int key[5] = {mixed(ctx) ? 1 : 0, dual ? 1 : 0, energy ? 1 : 0, ctx->cap, ctx->p3_warps};
+    if (std::memcmp(key, ctx->plan_key, sizeof key) != 0) {
+        CK(plan_p3bca(mixed(ctx), dual, energy, ctx->cap, ctx->p3_warps, &ctx->plan));
+        std::memcpy(ctx->plan_key, key, sizeof key);
+    }
     return TBMD_OK;
 }
 
@@ -351,9 +358,18 @@ static tbmd_status ensure_cells(tbmd_ctx *ctx, int64_t n, bool dual, bool energy
     struct {
         Grid g;
         int64_t cell_off[2], sys_off[2];
-    } tab = {ctx->grid, {0, ctx->grid.ncells}, {0, n}};
-    CK(ctx->gset_single.ensure(sizeof tab));
-    CK(cudaMemcpyAsync(ctx->gset_single.p, &tab, sizeof tab, cudaMemcpyHostToDevice, ctx->stream));
+    } tab;
+    std::memset(&tab, 0, sizeof tab);  // padding too: the table is compared bytewise below
+    tab.g = ctx->grid;
+    tab.cell_off[1] = ctx->grid.ncells;
+    tab.sys_off[1] = n;
+    static_assert(sizeof tab <= sizeof ctx->gset_host, "single-system table size");
+    if (!ctx->gset_single.p || std::memcmp(ctx->gset_host, &tab, sizeof tab) != 0) {
+        CK(ctx->gset_single.ensure(sizeof tab));
+        CK(cudaMemcpyAsync(ctx->gset_single.p, &tab, sizeof tab, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));  // tab lives on this stack frame
+        std::memcpy(ctx->gset_host, &tab, sizeof tab);
+    }
     char *base = ctx->gset_single.as<char>();
     ctx->gset = GridSet{(const Grid *)base, (const int64_t *)(base + offsetof(decltype(tab), cell_off)),
                         (const int64_t *)(base + offsetof(decltype(tab), sys_off)), 1};
@@ -595,7 +611,8 @@ void tbmd_destroy(tbmd_ctx *ctx)
     for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
     for (DevBuf *b : {&ctx->state, &ctx->snapshot, &ctx->scalars, &ctx->step_counts, &ctx->prefix, &ctx->partial,
                       &ctx->cell_n, &ctx->cell_c, &ctx->nbr_buf, &ctx->dirs, &ctx->hvp, &ctx->gset_single,
-                      &ctx->sweep_sys, &ctx->bpos, &ctx->bout, &ctx->bsys, &ctx->bprefix, &ctx->ncell_tab})
+                      &ctx->sweep_sys, &ctx->bpos, &ctx->bout, &ctx->bsys, &ctx->bprefix, &ctx->ncell_tab,
+                      &ctx->staging})
         b->release();
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -613,39 +630,53 @@ tbmd_status tbmd_set_particles(tbmd_ctx *ctx, int64_t n, const int32_t *id, cons
     const double *src[10] = {x, y, z, vx, vy, vz, ax, ay, az, m};
     for (int k = 0; k < 10; ++k)
         if (!src[k]) return fail(ctx, TBMD_INVALID_ARG, "null particle array %d", k);
-    for (int k = 0; k < 10; ++k)
-        if (!finite3(src[k], n)) return fail(ctx, TBMD_BAD_INPUT, "non-finite value in particle array %d", k);
-    for (int64_t i = 0; i < n; ++i)
-        if (!(m[i] > 0)) return fail(ctx, TBMD_BAD_INPUT, "mass of particle %lld is not positive", (long long)i);
     tbmd_status st = check_device(ctx);
     if (st != TBMD_OK) return st;
     CK(cudaStreamSynchronize(ctx->stream));
+    // The arrays go to a staging buffer and are checked there on the device (non-finite values,
+    // masses <= 0, extremes of x, y, z for the domain); the state is replaced only if they pass.
+    const size_t arr_bytes = sizeof(double) * 10 * (size_t)n;
+    CK(ctx->staging.ensure(arr_bytes + sizeof(ValidateResult) + 256));
+    double *stg = ctx->staging.as<double>();
+    ValidateResult *vr = (ValidateResult *)(ctx->staging.as<char>() + arr_bytes);
+    for (int k = 0; k < 10; ++k)
+        CK(cudaMemcpyAsync(stg + (size_t)k * n, src[k], sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    CK(launch_validate(n, stg, vr, sms * 4, ctx->stream));
+    ctx->launches += 1;
+    ValidateResult h{};
+    CK(cudaMemcpyAsync(&h, vr, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));  // the caller's arrays are free again from here
+    if (h.bad_arrays) {
+        int k = 0;
+        while (!(h.bad_arrays & (1u << k))) ++k;
+        return fail(ctx, TBMD_BAD_INPUT, "non-finite value in particle array %d", k);
+    }
+    if (h.bad_mass != ~0ull)
+        return fail(ctx, TBMD_BAD_INPUT, "mass of particle %lld is not positive", (long long)h.bad_mass);
     if (ctx->n != n) invalidate_graph(ctx);
     CK(ctx->state.ensure(sizeof(double) * 13 * (size_t)n));
     for (int k = 0; k < 13; ++k) ctx->s[k] = ctx->state.as<double>() + (size_t)k * n;
-    for (int k = 0; k < 10; ++k)
-        CK(cudaMemcpyAsync(ctx->s[k], src[k], sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->s[0], stg, arr_bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     CK(cudaMemsetAsync(ctx->s[10], 0, sizeof(double) * 3 * n, ctx->stream));
     ctx->id.resize(n);
-    for (int64_t i = 0; i < n; ++i) ctx->id[i] = id ? id[i] : (int32_t)i;
+    if (id) {
+        std::memcpy(ctx->id.data(), id, sizeof(int32_t) * n);
+    } else {
+        for (int64_t i = 0; i < n; ++i) ctx->id[i] = (int32_t)i;
+    }
     ctx->n = n;
     if (ctx->cfg.algorithm == TBMD_P3BCA) {
         // RegularGridDecomposition::getDomainMinMax + Init, from these (initial) positions
-        const double *p[3] = {x, y, z};
         for (int d = 0; d < 3; ++d) {
-            double mn = p[d][0], mxv = p[d][0];
-            for (int64_t i = 1; i < n; ++i) {
-                if (p[d][i] < mn) mn = p[d][i];
-                if (p[d][i] > mxv) mxv = p[d][i];
-            }
-            double a = mn - 0.0001, b = mxv + 0.0001;
+            const double a = key_to_double(h.min_key[d]) - 0.0001, b = key_to_double(h.max_key[d]) + 0.0001;
             ctx->lo[d] = a;
             ctx->L[d] = std::fabs(b - a);
         }
         ctx->domain_set = true;
         ctx->cap = 0;
     }
-    CK(cudaStreamSynchronize(ctx->stream));
     return TBMD_OK;
 }
 

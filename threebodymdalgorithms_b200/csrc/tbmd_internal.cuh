@@ -287,6 +287,18 @@ cudaError_t launch_predictor(int64_t n, double *x, double *y, double *z, const d
 cudaError_t launch_update(int64_t n, double *vx, double *vy, double *vz, double *ax, double *ay, double *az,
                           const double *fx, const double *fy, const double *fz, const double *m, double dt, double gx,
                           double gy, double gz, cudaStream_t st);
+// Result of the device-side input check of tbmd_set_particles (k_validate).
+struct ValidateResult {
+    unsigned int bad_arrays;  // bit k: array k holds a non-finite value
+    unsigned int pad;
+    unsigned long long bad_mass;    // smallest index with mass <= 0 (or NaN), ~0 if none
+    unsigned long long min_key[3];  // order-preserving keys of min / max of x, y, z
+    unsigned long long max_key[3];
+};
+// arrays: x y z vx vy vz ax ay az m, n each, back to back
+cudaError_t launch_validate(int64_t n, const double *arrays, ValidateResult *res, int grid, cudaStream_t st);
+double key_to_double(unsigned long long key);
+
 cudaError_t launch_record_count(unsigned long long *cur, unsigned long long *per_step, unsigned int *step,
                                 unsigned long long constant_count, cudaStream_t st);
 

@@ -29,6 +29,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstring>
 
 #include "tbmd_internal.cuh"
 
@@ -1187,6 +1188,77 @@ cudaError_t launch_record_count(unsigned long long *cur, unsigned long long *per
 {
     k_record_count<<<1, 1, 0, st>>>(cur, per_step, step, constant_count);
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Input check of tbmd_set_particles on the device: the particle arrays (x y z vx vy vz ax ay az m,
+// n each, back to back) are checked for non-finite values and non-positive masses, and the
+// extremes of x, y, z are reduced for the domain size.  Extremes travel as order-preserving
+// integer keys (exact), so the domain equals the one a host loop over the same values gives.
+__device__ __forceinline__ unsigned long long order_key(double d)
+{
+    const unsigned long long b = (unsigned long long)__double_as_longlong(d);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+__global__ void __launch_bounds__(256) k_validate(int64_t n, const double *__restrict__ a, ValidateResult *res)
+{
+    unsigned int bad = 0;
+    unsigned long long bad_mass = ~0ull;
+    unsigned long long mn[3] = {~0ull, ~0ull, ~0ull}, mx[3] = {0ull, 0ull, 0ull};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+#pragma unroll
+        for (int k = 0; k < 10; ++k) {
+            const double v = a[(int64_t)k * n + i];
+            if (!isfinite(v)) bad |= 1u << k;
+            if (k < 3) {
+                const unsigned long long key = order_key(v);
+                mn[k] = key < mn[k] ? key : mn[k];
+                mx[k] = key > mx[k] ? key : mx[k];
+            }
+            if (k == 9 && !(v > 0.0) && (unsigned long long)i < bad_mass) bad_mass = (unsigned long long)i;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+        const unsigned long long bm = __shfl_xor_sync(0xffffffffu, bad_mass, o);
+        bad_mass = bm < bad_mass ? bm : bad_mass;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const unsigned long long lo = __shfl_xor_sync(0xffffffffu, mn[k], o);
+            const unsigned long long hi = __shfl_xor_sync(0xffffffffu, mx[k], o);
+            mn[k] = lo < mn[k] ? lo : mn[k];
+            mx[k] = hi > mx[k] ? hi : mx[k];
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (bad) atomicOr(&res->bad_arrays, bad);
+        if (bad_mass != ~0ull) atomicMin(&res->bad_mass, bad_mass);
+        for (int k = 0; k < 3; ++k) {
+            atomicMin(&res->min_key[k], mn[k]);
+            atomicMax(&res->max_key[k], mx[k]);
+        }
+    }
+}
+
+cudaError_t launch_validate(int64_t n, const double *arrays, ValidateResult *res, int grid, cudaStream_t st)
+{
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(res, 0, sizeof(ValidateResult), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(&res->bad_mass, 0xff, 4 * sizeof(unsigned long long), st)) != cudaSuccess) return e;
+    const int64_t need = (n + 255) / 256;
+    k_validate<<<(unsigned)(need < grid ? need : grid), 256, 0, st>>>(n, arrays, res);
+    return cudaGetLastError();
+}
+
+double key_to_double(unsigned long long key)
+{
+    const unsigned long long b = (key >> 63) ? (key & 0x7fffffffffffffffull) : ~key;
+    double d;
+    std::memcpy(&d, &b, sizeof d);
+    return d;
 }
 
 }  // namespace tbmd
