@@ -93,6 +93,8 @@ struct tbmd_ctx {
     bool ncell_single = false;
     int max_stage = 256;  // neighbour staging capacity
     DevBuf cell_n, cell_c, nbr_buf;
+    DevBuf long_buf;      // chunk-pair items of long half lists
+    int long_cap = 0;     // capacity of long_buf in items
     int64_t cell_bufs_n = -1, cell_bufs_cells = -1;
     CellBufs cb{};
     int cap = 0;
@@ -309,11 +311,13 @@ static int initial_cap(const tbmd_ctx *ctx, int64_t n)
 static tbmd_status ensure_cell_bufs(tbmd_ctx *ctx, int64_t n, int64_t nc, bool dual, bool energy)
 {
     if (ctx->cell_bufs_n != n || ctx->cell_bufs_cells != nc) {
-        // per particle: FP64 xs ys zs dxs dys dzs fs[3] hs[3]; int32 cell_of, sorted, nbr_count
-        CK(ctx->cell_n.ensure((size_t)n * (12 * sizeof(double) + 3 * sizeof(int32_t)) + 256));
+        // per particle: float4 qhi qlo; FP64 xs ys zs dxs dys dzs fs[3] hs[3]; int32 cell_of, sorted, nbr_count
+        CK(ctx->cell_n.ensure((size_t)n * (2 * sizeof(float4) + 12 * sizeof(double) + 3 * sizeof(int32_t)) + 256));
         CK(ctx->cell_c.ensure((size_t)(3 * nc + 1) * sizeof(int32_t) + 256));
-        double *d = ctx->cell_n.as<double>();
         CellBufs &cb = ctx->cb;
+        cb.qhi = ctx->cell_n.as<float4>();
+        cb.qlo = cb.qhi + n;
+        double *d = (double *)(cb.qlo + n);
         cb.xs = d;
         cb.ys = d + n;
         cb.zs = d + 2 * n;
@@ -337,8 +341,14 @@ static tbmd_status ensure_cell_bufs(tbmd_ctx *ctx, int64_t n, int64_t nc, bool d
     }
     CK(ctx->nbr_buf.ensure((size_t)n * ctx->cap * sizeof(int32_t) + 64));
     ctx->cb.nbr = ctx->nbr_buf.as<int32_t>();
+    if (ctx->long_cap < 1024) ctx->long_cap = 1024;
+    CK(ctx->long_buf.ensure((size_t)ctx->long_cap * sizeof(unsigned long long)));
+    ctx->cb.long_items = ctx->long_buf.as<unsigned long long>();
+    ctx->cb.long_cap = ctx->long_cap;
     ctx->cb.max_count = (int32_t *)(ctx->scalars.as<char>() + 28);
-    ctx->cb.work_counter = (unsigned int *)(ctx->scalars.as<char>() + 32);
+    ctx->cb.work_counter = (unsigned int *)(ctx->scalars.as<char>() + 32);  // and + 36
+    ctx->cb.long_count = (unsigned int *)(ctx->scalars.as<char>() + 40);
+    ctx->cb.long_max = (unsigned int *)(ctx->scalars.as<char>() + 44);
     ctx->cb.cap = ctx->cap;
     const int key[5] = {mixed(ctx) ? 1 : 0, dual ? 1 : 0, energy ? 1 : 0, ctx->cap, ctx->p3_warps};
     if (std::memcmp(key, ctx->plan_key, sizeof key) != 0) {
@@ -612,7 +622,7 @@ void tbmd_destroy(tbmd_ctx *ctx)
     for (DevBuf *b : {&ctx->state, &ctx->snapshot, &ctx->scalars, &ctx->step_counts, &ctx->prefix, &ctx->partial,
                       &ctx->cell_n, &ctx->cell_c, &ctx->nbr_buf, &ctx->dirs, &ctx->hvp, &ctx->gset_single,
                       &ctx->sweep_sys, &ctx->bpos, &ctx->bout, &ctx->bsys, &ctx->bprefix, &ctx->ncell_tab,
-                      &ctx->staging})
+                      &ctx->staging, &ctx->long_buf})
         b->release();
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -713,13 +723,42 @@ tbmd_status tbmd_get_particles(tbmd_ctx *ctx, int32_t *id, double *x, double *y,
 }
 
 // Grow the neighbour capacity after an overflow; true if a retry is worthwhile.
-static bool grow_cap(tbmd_ctx *ctx, int32_t seen)
+// Overflow flags of the P3BCA lists: the longest list seen and the chunk-pair items requested.
+struct CapSeen {
+    int32_t max_count;
+    uint32_t pad[3];
+    uint32_t long_max;
+};
+static_assert(sizeof(CapSeen) == 20, "scalars 28..48");
+
+static cudaError_t reset_cap_flags(tbmd_ctx *ctx, cudaStream_t st)
 {
-    if (seen <= ctx->cap) return false;
-    int want = (int)((double)seen * 1.25) + 32;
-    ctx->cap = (want + 31) / 32 * 32;
-    invalidate_graph(ctx);
-    return true;
+    cudaError_t e = cudaMemsetAsync(ctx->scalars.as<char>() + 28, 0, 4, st);
+    if (e != cudaSuccess) return e;
+    return cudaMemsetAsync(ctx->scalars.as<char>() + 44, 0, 4, st);
+}
+
+static cudaError_t read_cap_flags(tbmd_ctx *ctx, cudaStream_t st, CapSeen *seen)
+{
+    return cudaMemcpyAsync(seen, ctx->scalars.as<char>() + 28, sizeof(CapSeen), cudaMemcpyDeviceToHost, st);
+}
+
+// Grow the list capacity or the chunk-pair item capacity after an overflow; true if a retry is
+// needed.
+static bool grow_caps(tbmd_ctx *ctx, const CapSeen &seen)
+{
+    bool grew = false;
+    if (seen.max_count > ctx->cap) {
+        int want = (int)((double)seen.max_count * 1.25) + 32;
+        ctx->cap = (want + 31) / 32 * 32;
+        grew = true;
+    }
+    if ((int64_t)seen.long_max > (int64_t)ctx->long_cap) {
+        ctx->long_cap = (int)((double)seen.long_max * 1.25) + 1024;
+        grew = true;
+    }
+    if (grew) invalidate_graph(ctx);
+    return grew;
 }
 
 tbmd_status tbmd_step(tbmd_ctx *ctx, int32_t iterations, uint64_t *counts)
@@ -739,10 +778,10 @@ tbmd_status tbmd_step(tbmd_ctx *ctx, int32_t iterations, uint64_t *counts)
     const bool cut = is_p3bca_cut(ctx);
     const int64_t n = ctx->n;
     for (int attempt = 0; attempt < 4; ++attempt) {
-        void *before[4] = {ctx->state.p, ctx->nbr_buf.p, ctx->cell_n.p, ctx->prefix.p};
+        void *before[5] = {ctx->state.p, ctx->nbr_buf.p, ctx->cell_n.p, ctx->prefix.p, ctx->long_buf.p};
         st = prepare(ctx, n, false, false);
         if (st != TBMD_OK) return st;
-        void *after[4] = {ctx->state.p, ctx->nbr_buf.p, ctx->cell_n.p, ctx->prefix.p};
+        void *after[5] = {ctx->state.p, ctx->nbr_buf.p, ctx->cell_n.p, ctx->prefix.p, ctx->long_buf.p};
         if (std::memcmp(before, after, sizeof before)) invalidate_graph(ctx);
         CK(cudaMemsetAsync(ctx->scalars.as<char>() + 8, 0, 56, ctx->stream));
         if (cut) {
@@ -766,13 +805,13 @@ tbmd_status tbmd_step(tbmd_ctx *ctx, int32_t iterations, uint64_t *counts)
             }
         }
         std::vector<unsigned long long> host(iterations);
-        int32_t seen = 0;
+        CapSeen seen{};
         CK(cudaMemcpyAsync(host.data(), ctx->step_counts.p, sizeof(unsigned long long) * iterations,
                            cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaMemcpyAsync(&seen, ctx->scalars.as<char>() + 28, sizeof seen, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(read_cap_flags(ctx, ctx->stream, &seen));
         CK(cudaStreamSynchronize(ctx->stream));
         phase_resolve(ctx);
-        if (cut && grow_cap(ctx, seen)) {
+        if (cut && grow_caps(ctx, seen)) {
             CK(cudaMemcpyAsync(ctx->s[0], ctx->snapshot.p, sizeof(double) * 9 * n, cudaMemcpyDeviceToDevice,
                                ctx->stream));
             continue;
@@ -792,7 +831,7 @@ static tbmd_status evaluate(tbmd_ctx *ctx, int64_t n, Pos pos, Out out, bool dua
     for (int attempt = 0; attempt < 4; ++attempt) {
         tbmd_status s = prepare(ctx, n, dual, energy != nullptr);
         if (s != TBMD_OK) return s;
-        CK(cudaMemsetAsync(ctx->scalars.as<char>() + 28, 0, 4, st));
+        CK(reset_cap_flags(ctx, st));
         if (energy) CK(cudaMemsetAsync(energy, 0, sizeof(double), st));
         if (count) CK(cudaMemsetAsync(count, 0, sizeof(unsigned long long), st));
         int nl = 0;
@@ -805,10 +844,10 @@ static tbmd_status evaluate(tbmd_ctx *ctx, int64_t n, Pos pos, Out out, bool dua
             phase_resolve(ctx);
         }
         if (!is_p3bca_cut(ctx)) return TBMD_OK;
-        int32_t seen = 0;
-        CK(cudaMemcpyAsync(&seen, ctx->scalars.as<char>() + 28, sizeof seen, cudaMemcpyDeviceToHost, st));
+        CapSeen seen{};
+        CK(read_cap_flags(ctx, st, &seen));
         CK(cudaStreamSynchronize(st));
-        if (!grow_cap(ctx, seen)) return TBMD_OK;
+        if (!grow_caps(ctx, seen)) return TBMD_OK;
     }
     return fail(ctx, TBMD_CAPACITY_RETRY, "neighbour capacity still exceeded after retries (cap %d)", ctx->cap);
 }
@@ -1205,7 +1244,7 @@ static tbmd_status batch_eval(tbmd_ctx *ctx, int32_t nsys, const int64_t *offset
             ctx->max_stage = stage;
             r = ensure_cell_bufs(ctx, N, all.ncells, dual, true);
             if (r != TBMD_OK) break;
-            CK(cudaMemsetAsync(ctx->scalars.as<char>() + 28, 0, 4, sm));
+            CK(reset_cap_flags(ctx, sm));
             CK(cudaMemsetAsync(E, 0, sizeof(double) * 2 * nsys, sm));
             CellBufs &cb = ctx->cb;
             CK(launch_cell_build(N, pos, ctx->grid, ctx->gset, cb, dual, sm, &nl));
@@ -1217,11 +1256,11 @@ static tbmd_status batch_eval(tbmd_ctx *ctx, int32_t nsys, const int64_t *offset
             CK(launch_p3bca(mx, dual, true, N, ctx->grid, ctx->gset, cb, nu, E, CNT, ctx->plan, sm));
             CK(launch_unsort(N, cb, out, dual, sm));
             nl += 3 + (dual ? 1 : 0);
-            int32_t seen = 0;
-            CK(cudaMemcpyAsync(&seen, ctx->scalars.as<char>() + 28, sizeof seen, cudaMemcpyDeviceToHost, sm));
+            CapSeen seen{};
+            CK(read_cap_flags(ctx, sm, &seen));
             CK(cudaStreamSynchronize(sm));
             r = TBMD_OK;
-            if (!grow_cap(ctx, seen)) break;
+            if (!grow_caps(ctx, seen)) break;
             r = TBMD_CAPACITY_RETRY;
         }
         ctx->cap = saved_cap > ctx->cap ? saved_cap : ctx->cap;  // the next ensure_cells rebuilds the single grid

@@ -243,6 +243,10 @@ cudaError_t launch_nata(bool mixed, bool dual, int R, bool energy, int64_t n, Po
 cudaError_t launch_nata_reduce(bool dual, int64_t n, int nblocks, const double *partial, Out out, cudaStream_t st);
 
 // P3BCA pipeline
+// Half-list chunk of the P3BCA triplet kernel: lists of at most P3_CHUNK entries are one work item,
+// longer ones are split into chunk pairs.
+constexpr int P3_CHUNK = 64;
+
 struct CellBufs {
     int32_t *cell_of;      // [n] cell of each particle (input order)
     int32_t *cell_count;   // [ncells]
@@ -250,12 +254,19 @@ struct CellBufs {
     int32_t *cell_fill;    // [ncells]
     int32_t *sorted;       // [n] sorted slot -> original index
     double *xs, *ys, *zs;  // [n] positions in sorted order
+    float4 *qhi, *qlo;     // [n] sorted positions relative to the system's box corner lo, as FP32
+                           //     hi + lo parts (x, y, z, unused): the neighbour kernel's FP32 test
     double *dxs, *dys, *dzs;  // [n] adjoint direction in sorted order (or NULL)
     int32_t *nbr;          // [n * cap] half neighbour lists (sorted indices)
     int32_t *nbr_count;    // [n]
     int32_t *max_count;    // [1] largest list length seen (overflow detection)
-    unsigned int *work_counter;  // [1] dynamic item counter of the triplet kernel
+    unsigned int *work_counter;  // [2] dynamic item counters of the triplet kernel (particles, chunk pairs)
     int cap;
+    // lists longer than P3_CHUNK: (s << 32 | I << 16 | J) chunk-pair items, queued by the neighbour kernel
+    unsigned long long *long_items;  // [long_cap]
+    int long_cap;
+    unsigned int *long_count;  // [1] items queued by this evaluation (reset before the neighbour kernel)
+    unsigned int *long_max;    // [1] largest item total requested (overflow detection)
     double *fs[3];         // [n] forces in sorted order
     double *hs[3];         // [n] H*direction in sorted order (adjoint)
 };

@@ -535,16 +535,26 @@ __global__ void k_cell_scatter(int64_t n, const int32_t *__restrict__ cell_of, c
     sorted[start[c] + slot] = (int32_t)i;
 }
 
-// Positions (and the adjoint direction) in sorted order.
-__global__ void k_gather(int64_t n, const int32_t *__restrict__ sorted, Pos pos, double *xs, double *ys, double *zs,
-                         double *dxs, double *dys, double *dzs)
+// Positions (and the adjoint direction) in sorted order, plus the FP32 hi/lo copy relative to the
+// system's box corner.
+__global__ void k_gather(int64_t n, const int32_t *__restrict__ sorted, Pos pos, const __grid_constant__ Grid g,
+                         GridSet set, double *xs, double *ys, double *zs, float4 *qhi, float4 *qlo, double *dxs,
+                         double *dys, double *dzs)
 {
     int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     int32_t i = sorted[s];
-    xs[s] = pos.x[i];
-    ys[s] = pos.y[i];
-    zs[s] = pos.z[i];
+    const double x = pos.x[i], y = pos.y[i], z = pos.z[i];
+    xs[s] = x;
+    ys[s] = y;
+    zs[s] = z;
+    const Grid &G = set.nsys > 1 ? set.grids[system_of(set.sys_off, set.nsys, s)] : g;
+    float hx, hy, hz, lx, ly, lz;
+    split<float>(x - G.lo[0], 0.0, hx, lx);
+    split<float>(y - G.lo[1], 0.0, hy, ly);
+    split<float>(z - G.lo[2], 0.0, hz, lz);
+    qhi[s] = make_float4(hx, hy, hz, 0.f);
+    qlo[s] = make_float4(lx, ly, lz, 0.f);
     if (dxs) {
         dxs[s] = pos.dx[i];
         dys[s] = pos.dy[i];
@@ -564,41 +574,53 @@ cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, const GridSet &
     k_cell_assign<<<nb, 256, 0, st>>>(n, pos.x, pos.y, pos.z, g, set, cb.cell_of, cb.cell_count);
     k_cell_scan<<<1, 1024, 0, st>>>(g.ncells, cb.cell_count, cb.cell_start);
     k_cell_scatter<<<nb, 256, 0, st>>>(n, cb.cell_of, cb.cell_start, cb.cell_fill, cb.sorted);
-    k_gather<<<nb, 256, 0, st>>>(n, cb.sorted, pos, cb.xs, cb.ys, cb.zs, with_dir ? cb.dxs : nullptr,
-                                 with_dir ? cb.dys : nullptr, with_dir ? cb.dzs : nullptr);
+    k_gather<<<nb, 256, 0, st>>>(n, cb.sorted, pos, g, set, cb.xs, cb.ys, cb.zs, cb.qhi, cb.qlo,
+                                 with_dir ? cb.dxs : nullptr, with_dir ? cb.dys : nullptr, with_dir ? cb.dzs : nullptr);
     if (launches) *launches += 4;
     return cudaGetLastError();
 }
 
 // Half neighbour lists: for sorted particle s, every t > s in the 27 (fewer on one-cell axes)
-// neighbouring cells with periodic d^2 <= cutoff^2 (exact FP64 test).
+// neighbouring cells with periodic d^2 <= cutoff^2 (the reference's test, structs.hpp:106-115,
+// d == cutoff inside).
 //
 // Block per cell c.  Particles are counting-sorted by cell id, so the candidates t > s of a
 // particle s in c are: the particles of c after s, and all particles of the neighbour cells with
 // id > c.  nbr_cells (built on the host with the grid) lists, per cell, its neighbour cells with
-// id >= c in increasing id order (-1 padded to 27).  The block scans their sizes, stages their
-// particles (positions and sorted indices) in shared memory in that order - cell by cell, so every
-// copy is coalesced - and the candidates of the i-th particle of c are the suffix after i.  Warps
-// take the particles of c in turn and sweep their suffix 32 candidates at a time, writing survivors
-// compacted by ballot.  A cell whose candidates exceed the staging capacity reads them from global
-// memory instead.  Lists longer than cap are truncated; the largest length is recorded so the host
-// can enlarge cap and recompute.
+// id >= c in increasing id order (-1 padded to 27).  The block scans their sizes and stages their
+// particles (FP32 hi/lo positions relative to the box corner, and sorted indices) in shared memory
+// in that order - cell by cell, so every copy is coalesced - and the candidates of the i-th
+// particle of c are the suffix after i.  Warps take the particles of c in turn and sweep their
+// suffix 32 candidates at a time, writing survivors compacted by ballot.  A cell whose candidates
+// exceed the staging capacity reads them from global memory instead.  Lists longer than cap are
+// truncated; the largest length is recorded so the host can enlarge cap and recompute.
+//
+// The test runs in FP32 on d = (hi_t - hi_s) + (lo_t - lo_s), which is within 2^-24 (|d| + L) of
+// the FP64 difference per component, inside the bound e = 16 eps32 (L + cutoff) of the guard band
+// (the triplet kernel's).  Outside the band around cutoff^2 the FP32 value decides; inside it the
+// exact FP64 test on the FP64 positions does, so the lists are exactly the reference's.  The
+// periodic form min(|d|, L - |d|) is always evaluated: positions are not wrapped into the box, so a
+// particle that drifted out of it sits in a cell at the other end with a raw offset near L.
 constexpr int NB_THREADS = 128;
+constexpr size_t NB_STAGE_BYTES = 2 * sizeof(float4) + sizeof(int32_t);  // per staged candidate
 
 __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant__ Grid g, GridSet set,
                                                           const int32_t *__restrict__ nbr_cells,
+                                                          const float4 *__restrict__ qhi,
+                                                          const float4 *__restrict__ qlo,
                                                           const double *__restrict__ xs,
                                                           const double *__restrict__ ys,
                                                           const double *__restrict__ zs,
                                                           const int32_t *__restrict__ cell_start, int32_t *nbr,
                                                           int32_t *nbr_count, int32_t *max_count, int cap,
-                                                          int max_stage)
+                                                          int max_stage, unsigned long long *long_items,
+                                                          unsigned int long_cap, unsigned int *long_count,
+                                                          unsigned int *long_max)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    double *sx = (double *)smraw;
-    double *sy = sx + max_stage;
-    double *sz = sy + max_stage;
-    int32_t *st = (int32_t *)(sz + max_stage);
+    float4 *shi = (float4 *)smraw;
+    float4 *slo = shi + max_stage;
+    int32_t *st = (int32_t *)(slo + max_stage);
     __shared__ int cstart[32], cpre[33];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int NW = NB_THREADS / 32;
@@ -607,6 +629,8 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
         if (b0 == e0) continue;
         const int sys = system_of(set.cell_off, set.nsys, c);
         const Grid &G = set.nsys > 1 ? set.grids[sys] : g;
+        const float Lx = (float)G.L[0], Ly = (float)G.L[1], Lz = (float)G.L[2];
+        const float sq_lo = (float)G.sqcut - G.band, sq_hi = (float)G.sqcut + G.band;
         if (warp == 0) {
             const int nc = lane < 27 ? nbr_cells[c * 27 + lane] : -1;
             const int cs = nc >= 0 ? cell_start[nc] : 0;
@@ -630,9 +654,8 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
                 if (len == 0) continue;
                 for (int i = threadIdx.x; i < len; i += NB_THREADS) {
                     const int t = cstart[k] + i;
-                    sx[beg + i] = xs[t];
-                    sy[beg + i] = ys[t];
-                    sz[beg + i] = zs[t];
+                    shi[beg + i] = qhi[t];
+                    slo[beg + i] = qlo[t];
                     st[beg + i] = t;
                 }
             }
@@ -640,7 +663,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
         __syncthreads();
         for (int sl = warp; sl < e0 - b0; sl += NW) {
             const int s = b0 + sl;  // cell c comes first in the candidate order: q = sl
-            const double xa = staged ? sx[sl] : xs[s], ya = staged ? sy[sl] : ys[s], za = staged ? sz[sl] : zs[s];
+            const float4 oh = staged ? shi[sl] : qhi[s], ol = staged ? slo[sl] : qlo[s];
             int cnt = 0;
             int32_t *dst = nbr + (int64_t)s * cap;
             for (int q0 = sl + 1; q0 < T; q0 += 32) {
@@ -648,21 +671,26 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
                 bool pass = false;
                 int t = 0;
                 if (q < T) {
-                    double x, y, z;
+                    float4 h, l;
                     if (staged) {
                         t = st[q];
-                        x = sx[q];
-                        y = sy[q];
-                        z = sz[q];
+                        h = shi[q];
+                        l = slo[q];
                     } else {
                         int k = 0;
                         while (k < 26 && cpre[k + 1] <= q) ++k;
                         t = cstart[k] + (q - cpre[k]);
-                        x = xs[t];
-                        y = ys[t];
-                        z = zs[t];
+                        h = qhi[t];
+                        l = qlo[t];
                     }
-                    pass = sqdist_periodic(xa, ya, za, x, y, z, G) <= G.sqcut;
+                    const float dx = (h.x - oh.x) + (l.x - ol.x), dy = (h.y - oh.y) + (l.y - ol.y),
+                                dz = (h.z - oh.z) + (l.z - ol.z);
+                    const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
+                    const float mx = fminf(ax, Lx - ax), my = fminf(ay, Ly - ay), mz = fminf(az, Lz - az);
+                    const float d2 = fmaf(mx, mx, fmaf(my, my, mz * mz));
+                    pass = d2 <= sq_lo;
+                    if (!pass && d2 <= sq_hi)
+                        pass = sqdist_periodic(xs[s], ys[s], zs[s], xs[t], ys[t], zs[t], G) <= G.sqcut;
                 }
                 const unsigned m = __ballot_sync(0xffffffffu, pass);
                 const int off = cnt + __popc(m & ((1u << lane) - 1u));
@@ -673,13 +701,34 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
                 nbr_count[s] = cnt;
                 atomicMax(max_count, cnt);
             }
+            // a list longer than one chunk: queue its chunk pairs (I <= J) for the triplet kernel
+            const int M = cnt < cap ? cnt : cap;
+            if (M > P3_CHUNK) {
+                const unsigned int nch = (unsigned int)((M + P3_CHUNK - 1) / P3_CHUNK);
+                const unsigned int nitems = nch * (nch + 1) / 2;
+                unsigned int base = 0;
+                if (lane == 0) {
+                    base = atomicAdd(long_count, nitems);
+                    atomicMax(long_max, base + nitems);
+                }
+                base = __shfl_sync(0xffffffffu, base, 0);
+                for (unsigned int k = lane; k < nitems; k += 32) {
+                    unsigned int I = 0, r = k;
+                    while (r >= nch - I) {
+                        r -= nch - I;
+                        ++I;
+                    }
+                    if (base + k < long_cap)
+                        long_items[base + k] = ((unsigned long long)(unsigned int)s << 32) | (I << 16) | (I + r);
+                }
+            }
         }
         __syncthreads();
     }
 }
 
 // Staging capacity: 2.5 times the expected candidate count (14 of the 27 cells have id >= c on
-// average), at least 256, at most 4096 (112 KiB).
+// average), at least 256, at most 4096 (144 KiB).
 int neighbor_stage_cap(const Grid &g, int64_t n)
 {
     const double mean = (double)n / (double)g.ncells;
@@ -723,20 +772,28 @@ cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, const
                              CellBufs &cb, cudaStream_t st)
 {
     (void)n;
-    const size_t smem = (size_t)max_stage * (3 * sizeof(double) + sizeof(int32_t));
+    const size_t smem = (size_t)max_stage * NB_STAGE_BYTES;
     int64_t blocks = g.ncells < 65535 * 16 ? g.ncells : 65535 * 16;
-    k_neighbors<<<(unsigned)blocks, NB_THREADS, smem, st>>>(g, set, nbr_cells, cb.xs, cb.ys, cb.zs, cb.cell_start,
-                                                            cb.nbr, cb.nbr_count, cb.max_count, cb.cap, max_stage);
+    cudaError_t e = cudaMemsetAsync(cb.long_count, 0, sizeof(unsigned int), st);
+    if (e != cudaSuccess) return e;
+    k_neighbors<<<(unsigned)blocks, NB_THREADS, smem, st>>>(g, set, nbr_cells, cb.qhi, cb.qlo, cb.xs, cb.ys, cb.zs,
+                                                            cb.cell_start, cb.nbr, cb.nbr_count, cb.max_count, cb.cap,
+                                                            max_stage, cb.long_items, (unsigned int)cb.long_cap,
+                                                            cb.long_count, cb.long_max);
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------------------------
-// P3BCA triplets.  Warp per sorted particle s (dynamic item counter).  Its half list (M slots) is
-// staged in the warp's shared memory: edge from s (hi, its square, and the lo part for the mixed
-// form), an S gradient accumulator per slot, the neighbour index and (FP64 forms) the neighbour's
-// FP64 position for the exact third-edge test.
+// P3BCA triplets.  A warp takes work items from two dynamic counters.  An item is a particle s
+// whose half list has at most P3_CHUNK (64) entries, or, for a longer list, a pair of its chunks
+// (I <= J) queued by the neighbour kernel; long lists are thus spread over many warps and the
+// shared memory of a warp is fixed (two chunks) whatever the list length.  The item's entries are
+// staged as slots in the warp's shared memory: edge from s (hi, its square, and the lo part for the
+// mixed form), an S gradient accumulator per slot, the neighbour index and (FP64 forms) the
+// neighbour's FP64 position for the exact third-edge test.
 //
-// Every unordered slot pair is visited once, block by block (blocks of 32 slots).  For own block A
+// Every unordered slot pair of the item (all pairs of one chunk, or all pairs across two chunks)
+// is visited once, block by block (blocks of 32 slots).  For own block A
 // lane x owns slot A+x: its edge and its gradient accumulator live in registers.
 //   - pairs inside A: circular diagonals, pair (x, (x + d) mod m_A), d = 1 .. m_A/2 (on the half
 //     diagonal of an even m_A only x < m_A/2);
@@ -744,8 +801,8 @@ cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, const
 //     t = 0..31; otherwise each slot of B in turn against all lanes.
 // In every warp step the partner slots are distinct, so partner gradients are added to their slot
 // with a plain shared-memory read-modify-write (one __syncwarp per step, no atomics); in the
-// broadcast steps the partner gradient is first summed over the warp.  The i-side gradient stays
-// in registers.  At the end each slot is flushed with one FP64 atomic.
+// broadcast steps the partner gradient is first summed over the warp.  The own-slot gradient stays
+// in registers.  At the end of an item each slot is flushed with one FP64 atomic.
 //
 // Cutoff test of the third edge.  FP64 forms: the reference's exact FP64 test (structs.hpp:106-115)
 // on the staged positions.  Mixed form: the same periodic formula in FP32 on the accurate third
@@ -761,7 +818,7 @@ struct alignas(4 * sizeof(S)) Slot4 {
 
 template <class S>
 struct SlotLayout {
-    // per-warp shared memory, [cap] of each: edge hi + b (Slot4), edge lo (Slot4, mixed only),
+    // per-warp shared memory, [2 * P3_CHUNK] of each: edge hi + b (Slot4), edge lo (Slot4, mixed only),
     // gradient accumulator (3 S), neighbour index, FP64 position (3 doubles, FP64 forms only)
     static constexpr bool mixed = HasLo<S>::value;
     static constexpr int nlo = mixed ? 1 : 0;
@@ -817,26 +874,27 @@ __device__ __forceinline__ bool cut_inside(const P3Warp<S> &W, const CellBufs &c
 
 template <class S, bool ENERGY>
 __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, CellBufs cb, double nu_d,
-                        double *energy_out, unsigned long long *count_out, unsigned int *counter)
+                        double *energy_out, unsigned long long *count_out)
 {
     using Acc = typename Traits<S>::Acc;
     using L = SlotLayout<S>;
+    constexpr int SL = 2 * P3_CHUNK;  // staged slots per warp: one or two chunks of a half list
     extern __shared__ __align__(16) unsigned char smem[];
     const int cap = cb.cap;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    unsigned char *base = smem + (size_t)wib * cap * L::bytes_per_slot;
+    unsigned char *base = smem + (size_t)wib * SL * L::bytes_per_slot;
     P3Warp<S> W;
     W.sd = (Slot4<S> *)base;
-    W.sl = W.sd + cap;
-    double *pbase = (double *)(W.sl + (L::nlo ? cap : 0));
+    W.sl = W.sd + SL;
+    double *pbase = (double *)(W.sl + (L::nlo ? SL : 0));
     W.px = pbase;
-    W.py = pbase + (L::npos ? cap : 0);
-    W.pz = W.py + (L::npos ? cap : 0);
-    W.gx = (S *)(W.pz + (L::npos ? cap : 0));
-    W.gy = W.gx + cap;
-    W.gz = W.gy + cap;
-    W.idx = (int32_t *)(W.gz + cap);
+    W.py = pbase + (L::npos ? SL : 0);
+    W.pz = W.py + (L::npos ? SL : 0);
+    W.gx = (S *)(W.pz + (L::npos ? SL : 0));
+    W.gy = W.gx + SL;
+    W.gz = W.gy + SL;
+    W.idx = (int32_t *)(W.gz + SL);
 
     const S nu = constant<S>(nu_d), nu3 = constant<S>(-3.0 * nu_d), nu15 = constant<S>(15.0 * nu_d);
     const Out outs = {cb.fs[0], cb.fs[1], cb.fs[2], cb.hs[0], cb.hs[1], cb.hs[2]};
@@ -857,13 +915,12 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
         }
     };
 
-    unsigned int w = 0;
-    if (lane == 0) w = atomicAdd(counter, 1u);
-    w = __shfl_sync(0xffffffffu, w, 0);
-    while ((int64_t)w < n) {
-        unsigned int wn = 0;
-        if (lane == 0) wn = atomicAdd(counter, 1u);
-        const int s = (int)w;
+    // One work item of particle s: list entries [offI, offI + mI) staged as slots [0, mI) and, for
+    // a pair of chunks, entries [offJ, offJ + mJ) as slots [mI, mI + mJ).  mJ == 0: every slot pair
+    // inside [0, mI); mJ > 0: every pair (a in [0, mI), b in [mI, mI + mJ)).  The item's gradients
+    // go out with one FP64 atomic per slot; s's share is minus their sum (translation invariance,
+    // per triplet, so per item).
+    auto item = [&](int s, int offI, int mI, int offJ, int mJ) {
         const int sys = system_of(set.sys_off, set.nsys, s);
         if (sys != cur_sys) {
             flush(cur_sys);
@@ -872,13 +929,13 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
         const Grid &G = set.nsys > 1 ? set.grids[sys] : g;
         const float Lx = (float)G.L[0], Ly = (float)G.L[1], Lz = (float)G.L[2];
         const float sq_lo = (float)G.sqcut - G.band, sq_hi = (float)G.sqcut + G.band;
-        const int raw_ok = G.raw_ok;
-        const int M = min(cb.nbr_count[s], cap);
+        const int Ms = mI + mJ;
         const double xi = cb.xs[s], yi = cb.ys[s], zi = cb.zs[s];
         const double dxi = dual ? cb.dxs[s] : 0.0, dyi = dual ? cb.dys[s] : 0.0, dzi = dual ? cb.dzs[s] : 0.0;
         bool nowrap = true;
-        for (int e = lane; e < M; e += 32) {
-            const int32_t t = cb.nbr[(int64_t)s * cap + e];
+        for (int e = lane; e < Ms; e += 32) {
+            const int pos_in_list = e < mI ? offI + e : offJ + (e - mI);
+            const int32_t t = cb.nbr[(int64_t)s * cap + pos_in_list];
             W.idx[e] = t;
             const double x = cb.xs[t], y = cb.ys[t], z = cb.zs[t];
             if (L::npos) {
@@ -898,12 +955,12 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
             W.gy[e] = szero<S>();
             W.gz[e] = szero<S>();
         }
-        const bool rawok = raw_ok && __all_sync(0xffffffffu, nowrap);
+        const bool rawok = G.raw_ok && __all_sync(0xffffffffu, nowrap);
         __syncwarp();
         S en = szero<S>();
 
-        for (int A0 = 0; A0 < M; A0 += 32) {
-            const int mA = min(32, M - A0);
+        for (int A0 = 0; A0 < mI; A0 += 32) {
+            const int mA = min(32, mI - A0);
             const bool own = lane < mA;
             const int a = A0 + (own ? lane : 0);
             const Slot4<S> od = W.sd[a];
@@ -938,23 +995,25 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
                 return gb;
             };
 
-            // pairs inside block A: circular diagonals
-            for (int d = 1; 2 * d <= mA; ++d) {
-                int y = lane + d;
-                if (y >= mA) y -= mA;
-                const bool act = own && (2 * d < mA || lane < d);
-                const int b = A0 + (y < mA ? y : 0);  // lanes past the block read a valid slot, masked
-                const V3<S> gb = pair(act, b);
-                if (act) {
-                    W.gx[b] = W.gx[b] + gb.x;
-                    W.gy[b] = W.gy[b] + gb.y;
-                    W.gz[b] = W.gz[b] + gb.z;
+            if (mJ == 0) {
+                // pairs inside block A: circular diagonals
+                for (int d = 1; 2 * d <= mA; ++d) {
+                    int y = lane + d;
+                    if (y >= mA) y -= mA;
+                    const bool act = own && (2 * d < mA || lane < d);
+                    const int b = A0 + (y < mA ? y : 0);  // lanes past the block read a valid slot, masked
+                    const V3<S> gb = pair(act, b);
+                    if (act) {
+                        W.gx[b] = W.gx[b] + gb.x;
+                        W.gy[b] = W.gy[b] + gb.y;
+                        W.gz[b] = W.gz[b] + gb.z;
+                    }
+                    __syncwarp();
                 }
-                __syncwarp();
             }
-            // pairs A x B with every later block
-            for (int B0 = A0 + 32; B0 < M; B0 += 32) {
-                const int mB = min(32, M - B0);
+            // pairs A x B with every later block B (of the same chunk, or of the second chunk)
+            for (int B0 = (mJ == 0 ? A0 + 32 : mI); B0 < Ms; B0 += 32) {
+                const int mB = min(32, Ms - B0);
                 if (mB >= 24) {
                     for (int t = 0; t < 32; ++t) {
                         const int y = (lane + t) & 31;
@@ -990,9 +1049,9 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
             __syncwarp();
         }
 
-        // flush the slots; i's gradient is minus the sum of all slot gradients (translation invariance)
+        // flush the slots; s's gradient is minus the sum of all slot gradients
         V3<Acc> gia = widen(vzero<S>());
-        for (int e = lane; e < M; e += 32) {
+        for (int e = lane; e < Ms; e += 32) {
             const V3<Acc> ge = widen(V3<S>{W.gx[e], W.gy[e], W.gz[e]});
             atomic_out(outs, W.idx[e], ge);
             gia = gia + ge;
@@ -1001,6 +1060,33 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
         if (lane == 0) atomic_out(outs, s, V3<Acc>{-gia.x, -gia.y, -gia.z});
         if (ENERGY) en_acc = en_acc + to_acc(en);
         __syncwarp();
+    };
+
+    // lists of at most one chunk: one item per particle
+    unsigned int w = 0;
+    if (lane == 0) w = atomicAdd(cb.work_counter, 1u);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    while ((int64_t)w < n) {
+        unsigned int wn = 0;
+        if (lane == 0) wn = atomicAdd(cb.work_counter, 1u);
+        const int s = (int)w;
+        const int M = min(cb.nbr_count[s], cap);
+        if (M <= P3_CHUNK && M > 1) item(s, 0, M, 0, 0);
+        w = __shfl_sync(0xffffffffu, wn, 0);
+    }
+    // longer lists: the chunk-pair items the neighbour kernel queued
+    const unsigned int nlong = min(*cb.long_count, (unsigned int)cb.long_cap);
+    if (lane == 0) w = atomicAdd(cb.work_counter + 1, 1u);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    while (w < nlong) {
+        unsigned int wn = 0;
+        if (lane == 0) wn = atomicAdd(cb.work_counter + 1, 1u);
+        const unsigned long long it = cb.long_items[w];
+        const int s = (int)(it >> 32), I = (int)((it >> 16) & 0xffffu), J = (int)(it & 0xffffu);
+        const int M = min(cb.nbr_count[s], cap);
+        const int mI = min(P3_CHUNK, M - I * P3_CHUNK);
+        const int mJ = J != I ? min(P3_CHUNK, M - J * P3_CHUNK) : 0;
+        item(s, I * P3_CHUNK, mI, J * P3_CHUNK, mJ);
         w = __shfl_sync(0xffffffffu, wn, 0);
     }
     flush(cur_sys);
@@ -1043,7 +1129,8 @@ static cudaError_t plan_p3bca_t(bool energy, int cap, int warps, P3Plan *plan)
     cudaError_t e;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    const size_t per_warp = (size_t)cap * SlotLayout<S>::bytes_per_slot;
+    (void)cap;
+    const size_t per_warp = (size_t)2 * P3_CHUNK * SlotLayout<S>::bytes_per_slot;
     const size_t smem_cap = 200 * 1024;
     if (warps < 1) warps = 1;
     while (warps > 1 && per_warp * warps > smem_cap) --warps;
@@ -1065,7 +1152,7 @@ cudaError_t plan_p3bca(bool mixed, bool dual, bool energy, int cap, int warps, P
 {
     // the neighbour kernel's largest staging size (4096 candidates), set once outside any capture
     cudaError_t e0 = cudaFuncSetAttribute(k_neighbors, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)(4096 * (3 * sizeof(double) + sizeof(int32_t))));
+                                          (int)(4096 * NB_STAGE_BYTES));
     if (e0 != cudaSuccess) return e0;
     if (dual) {
         if (mixed) return plan_p3bca_t<Dual<float>>(energy, cap, warps, plan);
@@ -1080,11 +1167,11 @@ static cudaError_t launch_p3bca_t(bool energy, int64_t n, const Grid &g, const G
                                   double *eo, unsigned long long *co, const P3Plan &plan, cudaStream_t st)
 {
     cudaError_t e;
-    if ((e = cudaMemsetAsync(cb.work_counter, 0, sizeof(unsigned int), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(cb.work_counter, 0, 2 * sizeof(unsigned int), st)) != cudaSuccess) return e;
     if (energy)
-        k_p3bca<S, true><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, set, cb, nu, eo, co, cb.work_counter);
+        k_p3bca<S, true><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, set, cb, nu, eo, co);
     else
-        k_p3bca<S, false><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, set, cb, nu, eo, co, cb.work_counter);
+        k_p3bca<S, false><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, set, cb, nu, eo, co);
     return cudaGetLastError();
 }
 
