@@ -518,7 +518,8 @@ def run_reference(args, world, rank):
 
 
 # exact triplets per step of the full workloads (from the oracle; C1/C2 are C(N,3))
-WORKLOAD_TRIPLETS = {"c1": math.comb(512, 3), "c2": math.comb(8192, 3), "c3": 48272380}
+WORKLOAD_TRIPLETS = {"c1": math.comb(512, 3), "c2": math.comb(8192, 3), "c3": 48272380, "c3c15": 8583257,
+                     "c4": 7282646752}
 
 
 def main():
