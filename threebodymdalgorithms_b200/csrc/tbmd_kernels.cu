@@ -648,16 +648,22 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
         __syncthreads();
         const int T = cpre[32];
         const bool staged = T <= max_stage;
+        // candidate q lies in table entry k: the largest k with cpre[k] <= q (empty entries have
+        // cpre[k] == cpre[k + 1] and are skipped by taking the largest)
+        auto entry_of = [&](int q) {
+            int k = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1)
+                if (k + step < 27 && cpre[k + step] <= q) k += step;
+            return k;
+        };
         if (staged) {
-            for (int k = 0; k < 27; ++k) {
-                const int beg = cpre[k], len = cpre[k + 1] - beg;
-                if (len == 0) continue;
-                for (int i = threadIdx.x; i < len; i += NB_THREADS) {
-                    const int t = cstart[k] + i;
-                    shi[beg + i] = qhi[t];
-                    slo[beg + i] = qlo[t];
-                    st[beg + i] = t;
-                }
+            for (int q = threadIdx.x; q < T; q += NB_THREADS) {
+                const int k = entry_of(q);
+                const int t = cstart[k] + (q - cpre[k]);
+                shi[q] = qhi[t];
+                slo[q] = qlo[t];
+                st[q] = t;
             }
         }
         __syncthreads();
@@ -677,8 +683,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
                         h = shi[q];
                         l = slo[q];
                     } else {
-                        int k = 0;
-                        while (k < 26 && cpre[k + 1] <= q) ++k;
+                        const int k = entry_of(q);
                         t = cstart[k] + (q - cpre[k]);
                         h = qhi[t];
                         l = qlo[t];
