@@ -821,15 +821,50 @@ struct alignas(4 * sizeof(S)) Slot4 {
     S x, y, z, w;
 };
 
+// Gradient accumulator of a slot: three components; for float padded to 16 bytes so that the
+// per-step update is one vector load and one vector store (the FP64 forms stay unpadded, their
+// shared memory bounds the resident warps).
+template <class S>
+struct Grad {
+    S x, y, z;
+};
+template <>
+struct alignas(16) Grad<float> {
+    float x, y, z, w;
+};
+template <class S>
+__device__ __forceinline__ Grad<S> grad_zero()
+{
+    Grad<S> g;
+    g.x = szero<S>();
+    g.y = szero<S>();
+    g.z = szero<S>();
+    return g;
+}
+template <>
+__device__ __forceinline__ Grad<float> grad_zero<float>()
+{
+    return Grad<float>{0.f, 0.f, 0.f, 0.f};
+}
+template <class S>
+__device__ __forceinline__ void slot_add(Grad<S> &slot, V3<S> g)
+{
+    Grad<S> v = slot;
+    v.x = v.x + g.x;
+    v.y = v.y + g.y;
+    v.z = v.z + g.z;
+    slot = v;
+}
+
 template <class S>
 struct SlotLayout {
     // per-warp shared memory, [2 * P3_CHUNK] of each: edge hi + b (Slot4), edge lo (Slot4, mixed only),
-    // gradient accumulator (3 S), neighbour index, FP64 position (3 doubles, FP64 forms only)
+    // FP64 position (3 doubles, FP64 forms only), gradient accumulator (Grad), neighbour index
     static constexpr bool mixed = HasLo<S>::value;
     static constexpr int nlo = mixed ? 1 : 0;
     static constexpr int npos = mixed ? 0 : 3;
     static constexpr size_t bytes_per_slot =
-        (1 + nlo) * sizeof(Slot4<S>) + npos * sizeof(double) + 3 * sizeof(S) + sizeof(int32_t);
+        (1 + nlo) * sizeof(Slot4<S>) + npos * sizeof(double) + sizeof(Grad<S>) + sizeof(int32_t);
 };
 
 template <class S>
@@ -848,7 +883,7 @@ struct P3Warp {
     Slot4<S> *sd;  // hi edge + b
     Slot4<S> *sl;  // lo edge (mixed)
     double *px, *py, *pz;
-    S *gx, *gy, *gz;
+    Grad<S> *gr;  // gradient accumulators
     int32_t *idx;
 };
 
@@ -877,9 +912,37 @@ __device__ __forceinline__ bool cut_inside(const P3Warp<S> &W, const CellBufs &c
     return sqdist_periodic(W.px[a], W.py[a], W.pz[a], W.px[b], W.py[b], W.pz[b], g) <= g.sqcut;
 }
 
+// Register cap of the triplet kernel per form.  The mixed forces kernel fits in 64 registers (32
+// resident warps per SM at 4 warps per block); the others keep about what they need unconstrained.
 template <class S, bool ENERGY>
-__global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, CellBufs cb, double nu_d,
-                        double *energy_out, unsigned long long *count_out)
+struct P3MaxReg {
+    static constexpr int value = 128;
+};
+template <>
+struct P3MaxReg<float, false> {
+    static constexpr int value = 64;
+};
+template <>
+struct P3MaxReg<float, true> {
+    static constexpr int value = 72;
+};
+template <bool E>
+struct P3MaxReg<double, E> {
+    static constexpr int value = 80;
+};
+template <bool E>
+struct P3MaxReg<Dual<float>, E> {
+    static constexpr int value = E ? 96 : 80;
+};
+template <bool E>
+struct P3MaxReg<Dual<double>, E> {
+    static constexpr int value = E ? 168 : 128;
+};
+
+template <class S, bool ENERGY>
+__global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
+    k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, CellBufs cb, double nu_d, double *energy_out,
+            unsigned long long *count_out)
 {
     using Acc = typename Traits<S>::Acc;
     using L = SlotLayout<S>;
@@ -896,10 +959,8 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
     W.px = pbase;
     W.py = pbase + (L::npos ? SL : 0);
     W.pz = W.py + (L::npos ? SL : 0);
-    W.gx = (S *)(W.pz + (L::npos ? SL : 0));
-    W.gy = W.gx + SL;
-    W.gz = W.gy + SL;
-    W.idx = (int32_t *)(W.gz + SL);
+    W.gr = (Grad<S> *)(W.pz + (L::npos ? SL : 0));
+    W.idx = (int32_t *)(W.gr + SL);
 
     const S nu = constant<S>(nu_d), nu3 = constant<S>(-3.0 * nu_d), nu15 = constant<S>(15.0 * nu_d);
     const Out outs = {cb.fs[0], cb.fs[1], cb.fs[2], cb.hs[0], cb.hs[1], cb.hs[2]};
@@ -956,9 +1017,7 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
             split<S>(ddz, dual ? cb.dzs[t] - dzi : 0.0, v.z, l.z);
             W.sd[e] = Slot4<S>{v.x, v.y, v.z, dot3(v, v)};
             if (L::nlo) W.sl[e] = Slot4<S>{l.x, l.y, l.z, szero<S>()};
-            W.gx[e] = szero<S>();
-            W.gy[e] = szero<S>();
-            W.gz[e] = szero<S>();
+            W.gr[e] = grad_zero<S>();
         }
         const bool rawok = G.raw_ok && __all_sync(0xffffffffu, nowrap);
         __syncwarp();
@@ -1009,9 +1068,7 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
                     const int b = A0 + (y < mA ? y : 0);  // lanes past the block read a valid slot, masked
                     const V3<S> gb = pair(act, b);
                     if (act) {
-                        W.gx[b] = W.gx[b] + gb.x;
-                        W.gy[b] = W.gy[b] + gb.y;
-                        W.gz[b] = W.gz[b] + gb.z;
+                        slot_add(W.gr[b], gb);
                     }
                     __syncwarp();
                 }
@@ -1026,9 +1083,7 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
                         const int b = B0 + (y < mB ? y : 0);
                         const V3<S> gb = pair(act, b);
                         if (act) {
-                            W.gx[b] = W.gx[b] + gb.x;
-                            W.gy[b] = W.gy[b] + gb.y;
-                            W.gz[b] = W.gz[b] + gb.z;
+                            slot_add(W.gr[b], gb);
                         }
                         __syncwarp();
                     }
@@ -1037,9 +1092,7 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
                         const int b = B0 + y;
                         const V3<S> gb = warp_sum3s(pair(own, b));
                         if (lane == 0) {
-                            W.gx[b] = W.gx[b] + gb.x;
-                            W.gy[b] = W.gy[b] + gb.y;
-                            W.gz[b] = W.gz[b] + gb.z;
+                            slot_add(W.gr[b], gb);
                         }
                         __syncwarp();
                     }
@@ -1047,9 +1100,7 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
             }
             // merge the own accumulator into its slot
             if (own) {
-                W.gx[a] = W.gx[a] + acc.x;
-                W.gy[a] = W.gy[a] + acc.y;
-                W.gz[a] = W.gz[a] + acc.z;
+                slot_add(W.gr[a], acc);
             }
             __syncwarp();
         }
@@ -1057,7 +1108,8 @@ __global__ void k_p3bca(int64_t n, const __grid_constant__ Grid g, GridSet set, 
         // flush the slots; s's gradient is minus the sum of all slot gradients
         V3<Acc> gia = widen(vzero<S>());
         for (int e = lane; e < Ms; e += 32) {
-            const V3<Acc> ge = widen(V3<S>{W.gx[e], W.gy[e], W.gz[e]});
+            const Grad<S> gs = W.gr[e];
+            const V3<Acc> ge = widen(V3<S>{gs.x, gs.y, gs.z});
             atomic_out(outs, W.idx[e], ge);
             gia = gia + ge;
         }
