@@ -49,6 +49,8 @@ WORKLOADS = {
                box=10.0),
     "c4": dict(desc="P3BCA, N=262144 clustered Gaussian (256 clusters, sigma 1) in 64^3, cutoff 2",
                algorithm="p3bca", n=262144, cutoff=2.0, gen="clustered", box=64.0),
+    "c5": dict(desc="64 systems, N uniform in 512..4096 at density 2.048, batched AUTA and P3BCA (cutoff 2), "
+                    "forward and adjoint", algorithm="batch", n=0, cutoff=2.0, gen="batch"),
 }
 FLOP_PER_TRIPLET = 120  # the fixed, formulation-independent per-triplet credit (BASELINE convention)
 DT, G = 0.001, (0.0, -9.81, 0.0)
@@ -135,24 +137,31 @@ def dist_setup():
     return world, rank, local
 
 
-def allreduce_max(v, world):
+def _all_reduce(v, world, op):
+    """v reduced over all ranks (NCCL: on the GPU; gloo: on the CPU)."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def allreduce_max(v, world):
+    import torch.distributed as dist
+    return _all_reduce(v, world, dist.ReduceOp.MAX)
 
 
 def allreduce_sum(v, world):
-    if world == 1:
-        return v
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _all_reduce(v, world, dist.ReduceOp.SUM)
+
+
+def aggregate(triplets_rank, ms_rank, world):
+    """Replicas: the whole job's triplets (sum over ranks) and its time (the slowest rank)."""
+    return allreduce_sum(float(triplets_rank), world), allreduce_max(float(ms_rank), world)
 
 
 def barrier(world):
@@ -160,7 +169,8 @@ def barrier(world):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
 
 
 def timed_steps(ctx, steps, flush, torch, reset=None):
@@ -217,9 +227,9 @@ def run_ours(args, world, rank, local):
         with ClockSampler(local) as clk:
             times, counts, launches = timed_steps(ctx, args.steps, flush, torch, reset)
         barrier(world)
-        total_ms = allreduce_max(sum(times), world)
-        result[prec] = dict(times=times, counts=counts, total_ms=total_ms, launches=launches, clocks=clk.summary(),
-                            tuning=ctx.tuning())
+        trip_all, total_ms = aggregate(sum(counts), sum(times), world)
+        result[prec] = dict(times=times, counts=counts, total_ms=total_ms, trip_all=trip_all, launches=launches,
+                            clocks=clk.summary(), tuning=ctx.tuning())
         # per-phase device times of the same steps (eager mode, events between phases)
         ctx.set_profiling(True)
         timed_steps(ctx, min(args.steps, 10), flush, torch, reset)
@@ -228,7 +238,7 @@ def run_ours(args, world, rank, local):
 
     main = result[args.precision]
     trip_rank = float(sum(main["counts"]))
-    trip_all = allreduce_sum(trip_rank, world)
+    trip_all = main["trip_all"]
     value = trip_all / (main["total_ms"] * 1e-3)
     ms_per_step = main["total_ms"] / args.steps
 
@@ -323,7 +333,7 @@ def run_ours(args, world, rank, local):
         }
         if fp64 and args.precision != "fp64":
             f_ms = fp64["total_ms"] / args.steps
-            line["fp64"] = {"ms_per_step": f_ms, "value": trip_all / (fp64["total_ms"] * 1e-3),
+            line["fp64"] = {"ms_per_step": f_ms, "value": fp64["trip_all"] / (fp64["total_ms"] * 1e-3),
                             "triplets_per_step": float(np.mean(fp64["counts"])),
                             "phases_ms_per_step": {k: round(v["ms"] / max(v["calls"], 1), 5)
                                                    for k, v in fp64["phases"].items()},
@@ -419,6 +429,67 @@ def run_trajectory(args, local):
         },
         f"positions_rel_l2_mixed_vs_fp64_step{K}": pos_err,
     }
+    print(json.dumps(line), flush=True)
+
+
+def run_batch(args, local):
+    """C5: 64 independent systems, N uniform in 512..4096, each uniform at density 2.048, evaluated
+    in one batched call (one set of launches over all systems): mixed-precision forces/energy for
+    AUTA (no cutoff) and P3BCA (cutoff 2), and the batched adjoint of a force-matching loss
+    sum |f_mixed(nu) - f_FP64(1.1 nu)|^2 (gradients w.r.t. positions and nu).  Times are CUDA
+    events around the C-ABI calls, host-array copies included."""
+    import torch
+    from threebodymdalgorithms_b200 import Context, generators
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    rng = np.random.default_rng(926762934)
+    systems = []
+    for i in range(64):
+        n = int(rng.integers(512, 4097))
+        side = generators.box_for_density(n, 2.048)
+        systems.append(generators.uniform(n, (side,) * 3, seed0=926762934 + i))
+    offsets = np.cumsum([0] + [len(st["x"]) for st in systems]).astype(np.int64)
+    cat = {k: np.concatenate([st[k] for st in systems]) for k in ("x", "y", "z")}
+
+    def timed(fn, reps):
+        out = None
+        ms = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            out = fn()
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return out, min(ms)
+
+    res = {}
+    for algo, cut in (("p3bca", 2.0), ("auta", 0.0)):
+        mx = Context(algo, "mixed", cut, stream=C.c_void_p(stream.cuda_stream))
+        ref = Context(algo, "fp64", cut, nu=1.1, stream=C.c_void_p(stream.cuda_stream))
+        reps = max(1, min(args.steps, 3 if algo == "auta" else 20))
+        fwd = lambda: mx.batch_forces(offsets, cat["x"], cat["y"], cat["z"])
+        fwd()
+        (fx, fy, fz, e, cnt), f_ms = timed(fwd, reps)
+        target = ref.batch_forces(offsets, cat["x"], cat["y"], cat["z"])
+        g = [2.0 * (a - b) for a, b in zip((fx, fy, fz), target[:3])]
+        ge = np.zeros(len(systems))
+        adj = lambda: mx.batch_adjoint(offsets, cat["x"], cat["y"], cat["z"], g[0], g[1], g[2], ge)
+        adj()
+        _, a_ms = timed(adj, reps)
+        trips = int(cnt.sum())
+        res[algo] = {"cutoff": cut, "triplets": trips, "forward_ms": f_ms, "forward_triplets_per_s": trips / (f_ms * 1e-3),
+                     "adjoint_ms": a_ms, "adjoint_triplets_per_s": trips / (a_ms * 1e-3), "repeats": reps}
+        mx.close()
+        ref.close()
+    line = {"metric": "triplets/s", "mode": "batched", "workload": "c5: 64 systems, N uniform in 512..4096, density 2.048",
+            "n_systems": 64, "n_total": int(offsets[-1]), "precision": "mixed (FP64 target forces at 1.1 nu)",
+            "data": "synthetic (seeded uniform systems)", "timing": "CUDA events around the batched C-ABI calls, "
+            "host copies included; best of the repeats", **res}
     print(json.dumps(line), flush=True)
 
 
@@ -546,6 +617,9 @@ def main():
         return
     if args.trajectory > 0:
         run_trajectory(args, int(os.environ.get("LOCAL_RANK", "0")))
+        return
+    if args.workload == "c5":
+        run_batch(args, int(os.environ.get("LOCAL_RANK", "0")))
         return
     world, rank, local = dist_setup()
     try:
