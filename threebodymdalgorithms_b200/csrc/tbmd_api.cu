@@ -107,6 +107,8 @@ struct tbmd_ctx {
 
     // batched evaluation (tbmd_batch_*): packed positions/directions/outputs and system tables
     DevBuf bpos, bout, bsys, bprefix;
+    void *hpin = nullptr;  // pinned host buffer of batched results
+    size_t hpin_bytes = 0;
 
     // phase profiling (eager mode): marks recorded on the stream, resolved after each sync
     bool profiling = false;
@@ -624,6 +626,7 @@ void tbmd_destroy(tbmd_ctx *ctx)
                       &ctx->sweep_sys, &ctx->bpos, &ctx->bout, &ctx->bsys, &ctx->bprefix, &ctx->ncell_tab,
                       &ctx->staging, &ctx->long_buf})
         b->release();
+    if (ctx->hpin) cudaFreeHost(ctx->hpin);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1135,11 +1138,25 @@ extern "C" tbmd_status tbmd_autotune(tbmd_ctx *ctx, const char *cache_path)
 // domain, evaluated together: one sweep launch over all systems (no cutoff), or one cell build,
 // one neighbour pass and one triplet launch over all systems (P3BCA).
 
+// Results of a batched evaluation, in the context's pinned host buffer (valid until the next
+// batched call on the context).
 struct BatchResult {
-    std::vector<double> f, h;       // 3 * N each (h only for the adjoint)
-    std::vector<double> energy;     // nsys
-    std::vector<uint64_t> counts;   // nsys
+    double *f = nullptr, *h = nullptr;  // 3 * N each (h only for the adjoint)
+    double *energy = nullptr;           // nsys
+    std::vector<uint64_t> counts;       // nsys
 };
+
+// Pinned host memory of the context for batched results (device-to-host copies as direct DMA).
+static cudaError_t ensure_host_pinned(tbmd_ctx *ctx, size_t bytes)
+{
+    if (bytes <= ctx->hpin_bytes && ctx->hpin) return cudaSuccess;
+    if (ctx->hpin) cudaFreeHost(ctx->hpin);
+    ctx->hpin = nullptr;
+    ctx->hpin_bytes = 0;
+    cudaError_t e = cudaMallocHost(&ctx->hpin, bytes);
+    if (e == cudaSuccess) ctx->hpin_bytes = bytes;
+    return e;
+}
 
 static tbmd_status batch_eval(tbmd_ctx *ctx, int32_t nsys, const int64_t *offsets, const double *box,
                               const double *lo, const double *x, const double *y, const double *z, const double *gfx,
@@ -1307,19 +1324,18 @@ static tbmd_status batch_eval(tbmd_ctx *ctx, int32_t nsys, const int64_t *offset
         nl += 1;
     }
     ctx->launches += nl;
-    res.f.resize(3 * N);
-    res.energy.resize(nsys);
-    CK(cudaMemcpyAsync(res.f.data(), O, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, sm));
-    if (dual) {
-        res.h.resize(3 * N);
-        CK(cudaMemcpyAsync(res.h.data(), O + 3 * N, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, sm));
-    }
-    CK(cudaMemcpyAsync(res.energy.data(), E, sizeof(double) * nsys, cudaMemcpyDeviceToHost, sm));
+    CK(ensure_host_pinned(ctx, sizeof(double) * (6 * (size_t)N + nsys)));
+    res.f = (double *)ctx->hpin;
+    res.h = res.f + 3 * N;
+    res.energy = res.h + 3 * N;
+    CK(cudaMemcpyAsync(res.f, O, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, sm));
+    if (dual) CK(cudaMemcpyAsync(res.h, O + 3 * N, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, sm));
+    CK(cudaMemcpyAsync(res.energy, E, sizeof(double) * nsys, cudaMemcpyDeviceToHost, sm));
     CK(cudaStreamSynchronize(sm));
     if (ctx->cfg.nu == 0.0) {  // the nu = 1 parts were evaluated; the true f, E and H vanish
-        for (double &v : res.f) v = 0.0;
-        for (double &v : res.h) v = 0.0;
-        for (double &v : res.energy) v = 0.0;
+        std::fill(res.f, res.f + 3 * N, 0.0);
+        if (dual) std::fill(res.h, res.h + 3 * N, 0.0);
+        std::fill(res.energy, res.energy + nsys, 0.0);
     }
     return TBMD_OK;
 }
@@ -1334,7 +1350,7 @@ extern "C" tbmd_status tbmd_batch_forces(tbmd_ctx *ctx, int32_t nsys, const int6
     const int64_t N = offsets[nsys];
     double *o3[3] = {fx, fy, fz};
     for (int k = 0; k < 3; ++k)
-        if (o3[k]) std::memcpy(o3[k], r.f.data() + k * N, sizeof(double) * N);
+        if (o3[k]) std::memcpy(o3[k], r.f + k * N, sizeof(double) * N);
     for (int s = 0; s < nsys; ++s) {
         if (energy) energy[s] = r.energy[s];
         if (triplets) triplets[s] = r.counts[s];
@@ -1355,16 +1371,16 @@ extern "C" tbmd_status tbmd_batch_adjoint(tbmd_ctx *ctx, int32_t nsys, const int
     const double *g3[3] = {gfx, gfy, gfz};
     double *o3[3] = {gx, gy, gz};
     const double nu = ctx->cfg.nu;
-    std::vector<double> fe(3 * N, 0.0);
-    // with nu = 0 batch_eval zeroed f, E and H; g_nu needs the nu = 1 parts, recomputed below
+    // with nu = 0 batch_eval zeroed f, E and H (so gx = 0); g_nu needs the nu = 1 parts, recomputed
+    // here (into the same pinned buffer: f and E are replaced, h is no longer needed)
     if (nu == 0.0) {
         BatchResult r1;
         ctx->cfg.nu = 1.0;
         st = batch_eval(ctx, nsys, offsets, box, lo, x, y, z, nullptr, nullptr, nullptr, r1);
         ctx->cfg.nu = 0.0;
         if (st != TBMD_OK) return st;
-        r.f.swap(r1.f);
-        r.energy.swap(r1.energy);
+        r.f = r1.f;
+        r.energy = r1.energy;
     }
     for (int s = 0; s < nsys; ++s) {
         const double ge = g_energy[s];
