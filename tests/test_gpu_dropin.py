@@ -1,4 +1,6 @@
 """The drop-in executable against the reference executable's own CSV output (golden files)."""
+import json
+import math
 import subprocess
 from pathlib import Path
 
@@ -41,7 +43,15 @@ def test_cli_output_matches_reference(name, args, last, tmp_path):
 def test_cli_mixed_and_dump(tmp_path):
     run_main(["-a", "P3BCA", "-i", "2", "-c", "2", "-d", "0.001", "-gy", "-9.81", "-prec", "mixed",
               "-csv", str(GOLDEN / "p3bca_n512_c2_3steps.csv"), "-dumpfull", str(tmp_path / "d.txt"),
-              "-op", str(tmp_path / "prof.json")], tmp_path)
+              "-op", str(tmp_path / "prof.json"), "-opsteps", str(tmp_path / "steps.json")], tmp_path)
     lines = (tmp_path / "d.txt").read_text().splitlines()
     assert lines[0].startswith("step 0 buffer 1 triplets 12982")
-    assert (tmp_path / "prof.json").read_text().startswith("[{\"allTimes\"")
+    steps = [json.loads(line) for line in (tmp_path / "steps.json").read_text().splitlines()]
+    assert len(steps) == 2 and steps[0]["triplets"] == 12982 and steps[0]["max"] > 0
+    prof = json.loads((tmp_path / "prof.json").read_text())
+    # the reference's PROFILE_3BMDA document shape (main.cpp:127-451)
+    assert set(prof) == {"times", "hitrate", "hitrate per proc", "stvr"}
+    forces = prof["times"]["calculateForces"]
+    assert forces["time unit"] == "nanosecond" and len(forces["times per proc"]["0"]) == 2
+    assert all(t > 0 for t in forces["times per proc"]["0"])
+    assert prof["hitrate"]["avg hitrate per sim step"][0] == pytest.approx(12982 / math.comb(512, 3))

@@ -11,8 +11,11 @@
 // GPU options: -prec fp64|mixed, -nu V (AT strength, default 1.0 as main.cpp:41), -device N,
 // -nograph, -tune CACHE.JSONL (autotuner), -dumpfull FILE (state at %.17g after the run),
 // -parseonly (print the parsed arguments as JSON and exit without touching the GPU).
-// -op FILE writes per-step GPU timings as JSON (the reference's MEASURESIMSTEP_3BMDA line format,
-// Simulation.cpp:59-68, in nanoseconds).
+// -op FILE writes the profile document of the reference's PROFILE_3BMDA build (main.cpp:127-451):
+// "times" per timer (time unit, avg/total over ranks, per-rank lists), "hitrate" (triplets inside
+// over the C(N,3) candidates the reference's P=1 loop visits, per step), "hitrate per proc" and
+// "stvr", with the GPU phases as timers (one rank).  -opsteps FILE writes per-step times in the
+// MEASURESIMSTEP_3BMDA line format (Simulation.cpp:59-68, nanoseconds) plus the triplet count.
 //
 // Output (Simulation.cpp:74-79, utility.cpp:54-68): with -o base.csv, after every step i the file
 // base_<i>.csv with header "ID, pX, pY, pZ, vX, vY, vZ, aX, aY, aZ, m, fX, fY, fZ", rows sorted by
@@ -36,7 +39,7 @@ struct Args {
     int iterations = 0;
     double cutoff = 0.0;
     double deltaT = 0.0;
-    std::string inputCSV, outputCSV, outputProfile, benchYaml;
+    std::string inputCSV, outputCSV, outputProfile, outputSteps, benchYaml;
     int algorithm = TBMD_NATA;
     double g[3] = {0.0, 0.0, 0.0};
     bool optimalDecomposition = false;
@@ -63,14 +66,15 @@ void printHelp()
               << "\t-csv,--csv\t\tcsv file with particles\n"
               << "\t-o,--out\t\tcsv base file name that will be used to create all csv outputs from each "
                  "simulation step\n"
-              << "-op,--outProfile\t\tjson file to save per-step timings\n"
+              << "-op,--outProfile\t\tjson file to save profile output\n"
               << "-decomp,--decomp\t\t(optimal | naive) decomposition strategy for cart topology (ignored)\n"
               << "-benchyaml,--benchyaml\t\tYAML file that contains config for benchmarks (ignored)\n"
               << "\t-c,--cutoff\t\tcutoff distance\n"
               << "GPU options:\n"
               << "\t-prec\t\tfp64 | mixed\n\t-nu\t\tAT strength (1.0)\n\t-device\t\tCUDA device\n"
               << "\t-nograph\t\tno CUDA graph\n\t-tune\t\tautotuner cache file\n"
-              << "\t-dumpfull\t\twrite the final state with 17 digits\n\t-parseonly\t\tprint parsed args" << std::endl;
+              << "\t-dumpfull\t\twrite the final state with 17 digits\n\t-opsteps\t\tper-step timings (json lines)\n"
+              << "\t-parseonly\t\tprint parsed args" << std::endl;
 }
 
 [[noreturn]] void usageExit()
@@ -144,6 +148,8 @@ Args parse(const std::vector<std::string> &args)
                 a.tuneCache = value();
             } else if (isFlag(f, "dumpfull", "-dumpfull")) {
                 a.dumpFull = value();
+            } else if (isFlag(f, "opsteps", "-opsteps")) {
+                a.outputSteps = value();
             } else if (isFlag(f, "parseonly", "-parseonly")) {
                 a.parseOnly = true;
             } else if (isFlag(f, "h", "-help")) {
@@ -257,6 +263,39 @@ void writeFull(const std::string &path, const State &s, const std::vector<uint64
 
 }  // namespace
 
+// The PROFILE_3BMDA document (main.cpp:127-451) for one rank.  Timers are the GPU phases of a step
+// (device time per step, nanoseconds); the reference's force timer name "calculateForces" is the
+// triplet phase, and "simulationStep" is the host wall time of the whole step.  hitrate: triplets
+// inside over C(N,3), the candidates of the reference's P=1 loop (P3BCA.cpp:632-636, 790-794).
+// stvr of a single rank is 0.
+static void writeProfile(const std::string &path, const std::vector<std::vector<long long>> &phaseNs,
+                         const std::vector<long long> &stepNs, const std::vector<uint64_t> &counts, int64_t n)
+{
+    static const char *names[] = {"predictor", "cellBuild", "neighbourLists", "calculateForces", "update"};
+    std::ofstream o(path);
+    o << "{\"times\": {";
+    const size_t nphase = phaseNs.empty() ? 0 : std::min<size_t>(phaseNs[0].size(), 5);
+    for (size_t k = 0; k <= nphase; ++k) {
+        std::vector<long long> v;
+        for (size_t i = 0; i < stepNs.size(); ++i) v.push_back(k < nphase ? phaseNs[i][k] : stepNs[i]);
+        long long total = 0;
+        for (long long t : v) total += t;
+        const double avg = v.empty() ? 0.0 : (double)total / (double)v.size();
+        o << (k ? ", " : "") << "\"" << (k < nphase ? names[k] : "simulationStep")
+          << "\": {\"time unit\": \"nanosecond\", \"avg time all proc\": " << avg
+          << ", \"total time all proc\": " << (double)total << ", \"total avg time union proc\": " << (double)total
+          << ", \"total max time union proc\": " << total << ", \"times per proc\": {\"0\": [";
+        for (size_t i = 0; i < v.size(); ++i) o << (i ? ", " : "") << v[i];
+        o << "]}}";
+    }
+    const double cand = n >= 3 ? (double)n * (double)(n - 1) * (double)(n - 2) / 6.0 : 0.0;
+    std::ostringstream hr;
+    hr.precision(17);
+    for (size_t i = 0; i < counts.size(); ++i) hr << (i ? ", " : "") << (cand > 0 ? (double)counts[i] / cand : 0.0);
+    o << "}, \"hitrate\": {\"avg hitrate per sim step\": [" << hr.str() << "]}, \"hitrate per proc\": {\"0\": ["
+      << hr.str() << "]}, \"stvr\": [{\"rank\": [0], \"stvr\": 0.0}]}\n";
+}
+
 int main(int argc, char **argv)
 {
     std::vector<std::string> args(argv + 1, argv + argc);
@@ -314,34 +353,45 @@ int main(int argc, char **argv)
 
     std::vector<uint64_t> counts;
     std::vector<long long> stepNs;
+    std::vector<std::vector<long long>> phaseNs;  // [step][phase], device time of each GPU phase
     State s;
+    const bool profile = !a.outputProfile.empty();
     if (n > 0 && a.iterations > 0) {
-        const bool perStep = !a.outputCSV.empty() || !a.outputProfile.empty();
+        const bool perStep = !a.outputCSV.empty() || profile || !a.outputSteps.empty();
         if (perStep) {
             for (int i = 0; i < a.iterations; ++i) {
                 uint64_t c = 0;
+                if (profile && tbmd_set_profiling(ctx, 1) != TBMD_OK) die("set_profiling");  // resets the timers
                 auto t0 = std::chrono::steady_clock::now();
                 if (tbmd_step(ctx, 1, &c) != TBMD_OK) die("step");
                 auto t1 = std::chrono::steady_clock::now();
                 stepNs.push_back(std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count());
                 counts.push_back(c);
+                if (profile) {
+                    double ms[8];
+                    uint64_t calls[8], launches[8];
+                    const int np = tbmd_phase_times(ctx, ms, calls, launches, 8);
+                    std::vector<long long> row;
+                    for (int k = 0; k < np; ++k) row.push_back((long long)(ms[k] * 1e6 + 0.5));
+                    phaseNs.push_back(row);
+                }
                 if (!a.outputCSV.empty()) {
                     if (!fetch(ctx, n, s)) die("get_particles");
                     writeStepCSV(stepPath(a.outputCSV, i), s);
                 }
             }
+            if (profile) tbmd_set_profiling(ctx, 0);
         } else {
             counts.resize(a.iterations);
             if (tbmd_step(ctx, a.iterations, counts.data()) != TBMD_OK) die("step");
         }
     }
-    if (!a.outputProfile.empty()) {
-        std::ofstream prof(a.outputProfile);
-        prof << "[";
+    if (profile) writeProfile(a.outputProfile, phaseNs, stepNs, counts, n);
+    if (!a.outputSteps.empty()) {
+        std::ofstream prof(a.outputSteps);
         for (size_t i = 0; i < stepNs.size(); ++i)
-            prof << (i ? ", " : "") << "{\"allTimes\": [" << stepNs[i] << "], \"max\": " << stepNs[i]
-                 << ", \"triplets\": " << counts[i] << "}";
-        prof << "]\n";
+            prof << "{\"allTimes\": [" << stepNs[i] << "], \"max\": " << stepNs[i] << ", \"triplets\": " << counts[i]
+                 << "}\n";
     }
     if (!a.dumpFull.empty() && n > 0) {
         if (!fetch(ctx, n, s)) die("get_particles");
