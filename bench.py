@@ -56,12 +56,25 @@ FLOP_PER_TRIPLET = 120  # the fixed, formulation-independent per-triplet credit 
 DT, G = 0.001, (0.0, -9.81, 0.0)
 
 
-def make_input(w):
+def make_input(w, device=None):
+    """The workload's particles: the reference generator's sequence after its 6-digit CSV round trip.
+    With a device, generated on the GPU (tbmd_generate_particles) and read back; otherwise by the
+    host generator (the reference arm's path)."""
     from threebodymdalgorithms_b200 import generators as gen
+    side = w.get("box") or gen.box_for_density(w["n"], 2.048)
+    if device is not None:
+        from threebodymdalgorithms_b200 import Context
+        ctx = Context("auta", device=device)
+        if w["gen"] == "uniform":
+            ctx.generate(kind="uniform", n=w["n"], box=(side, side, side))
+        else:
+            ctx.generate(kind="clusteredgauss", n=w["n"], n_clusters=256, box=(side, side, side))
+        st = ctx.get_state()
+        ctx.close()
+        return {k: st[k] for k in ("id", "x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m")}
     if w["gen"] == "uniform":
-        side = w.get("box") or gen.box_for_density(w["n"], 2.048)
         return gen.as_csv_values(gen.uniform(w["n"], (side, side, side), 1.0))
-    return gen.as_csv_values(gen.clustered_gauss(w["n"], 256, (w["box"],) * 3, 0.0, 1.0, 1.0))
+    return gen.as_csv_values(gen.clustered_gauss(w["n"], 256, (side,) * 3, 0.0, 1.0, 1.0))
 
 
 class ClockSampler:
@@ -206,7 +219,7 @@ def run_ours(args, world, rank, local):
     # a dedicated stream: the library, the CUDA events and the L2 flush all run on it
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    st = make_input(w)
+    st = make_input(w, device=local)
     n = len(st["x"])
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -322,8 +335,8 @@ def run_ours(args, world, rank, local):
             "metric": "triplets/s", "value": value, "unit": "triplets/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 geometry + f64 accumulation" if args.precision == "mixed" else "f64",
-            "data": "synthetic: the reference's particlegenerator sequences (mt19937 seed 926762934), 6-digit CSV "
-                    "values; every timed step restarts from this input",
+            "data": "synthetic: the reference's particlegenerator sequences (mt19937 seed 926762934) after its 6-digit "
+                    "CSV round trip, generated on the device; every timed step restarts from this input",
             "config": {"workload": f"{args.workload}: {w['desc']}", "algorithm": w["algorithm"], "n": n,
                        "cutoff": w["cutoff"], "precision": args.precision, "dt": DT, "g": list(G),
                        "triplets_per_step": mean_trip, "l2": "flushed (256 MiB write) between timed steps",
@@ -355,7 +368,7 @@ def run_trajectory(args, local):
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    st = make_input(w)
+    st = make_input(w, device=local)
     n = len(st["x"])
     K = args.trajectory
 

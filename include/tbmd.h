@@ -94,6 +94,33 @@ tbmd_status tbmd_get_particles(tbmd_ctx *ctx, int32_t *id, double *x, double *y,
 
 int64_t tbmd_num_particles(const tbmd_ctx *ctx);
 
+/* Particle generation on the device (the reference's particlegenerator, src/tools/particleToCSV.cpp,
+ * UniformGenerator.cpp:12-28, ClusteredGaussGenerator.cpp:15-47), loaded as the context's particles
+ * like tbmd_set_particles: ids 0..n-1, the given velocity, zero acceleration, the given mass.
+ * Positions are the generator's exact sequence (std::mt19937 / std::minstd_rand0 with libstdc++'s
+ * distributions); with csv_digits = 6 every value is rounded to 6 significant digits, which is what
+ * the reference's main reads back from the generator's CSV. */
+typedef enum { TBMD_GEN_UNIFORM = 0, TBMD_GEN_CLUSTERED_GAUSS = 1 } tbmd_generator_kind;
+typedef struct {
+    int32_t kind;        /* tbmd_generator_kind (--generator uniform | clusteredgauss) */
+    int64_t n;           /* --numparticles; clustered: n / n_clusters particles per cluster */
+    double box[3];       /* --blx --bly --blz */
+    double corner[3];    /* bottomLeftCorner (not a generator flag; the tool's is 0, 0, 0) */
+    double velocity[3];  /* --vx --vy --vz */
+    double mass;         /* --mass */
+    uint32_t seed0;      /* --seed0 */
+    uint32_t seed1;      /* --seed1 (cluster centres) */
+    int32_t n_clusters;  /* --numclusters */
+    double mean;         /* --distmean */
+    double stddev;       /* --diststddev */
+    int32_t csv_digits;  /* 6: the CSV round trip; 0: exact doubles */
+    int32_t reserved[7];
+} tbmd_generator;
+/* Defaults: uniform, n 0, box 10^3, corner 0, velocity 0, mass 1, seeds 926762934 / 89347587 (the
+ * reference's documented seeds), 1 cluster, mean 0, stddev 1, csv_digits 6. */
+void tbmd_generator_init(tbmd_generator *gen);
+tbmd_status tbmd_generate_particles(tbmd_ctx *ctx, const tbmd_generator *gen);
+
 /* Simulation::Start for `iterations` steps (Simulation.cpp:28-81): per step predictor
  * (structs.hpp:40-55), force reset + triplet forces (Algorithm::SimulationStep), update
  * (structs.hpp:57-99).  triplets_per_step (may be NULL) receives, per step, the value the

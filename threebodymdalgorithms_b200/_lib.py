@@ -23,7 +23,8 @@ EXPORTS = ("tbmd_config_init", "tbmd_create", "tbmd_destroy", "tbmd_last_error",
            "tbmd_abi_version", "tbmd_set_particles", "tbmd_get_particles", "tbmd_num_particles", "tbmd_step",
            "tbmd_forces", "tbmd_adjoint", "tbmd_forces_device", "tbmd_adjoint_device", "tbmd_set_domain",
            "tbmd_cells", "tbmd_batch_forces", "tbmd_batch_adjoint", "tbmd_autotune", "tbmd_tuning", "tbmd_sync",
-           "tbmd_kernel_launches", "tbmd_set_profiling", "tbmd_phase_times", "tbmd_nata_forces_noalloc")
+           "tbmd_kernel_launches", "tbmd_set_profiling", "tbmd_phase_times", "tbmd_nata_forces_noalloc",
+           "tbmd_generator_init", "tbmd_generate_particles")
 PHASES = ("predictor", "cells", "neighbors", "triplets", "update")
 
 
@@ -38,6 +39,16 @@ class Config(C.Structure):
                 ("g", C.c_double * 3), ("nu", C.c_double), ("device", C.c_int32), ("use_graph", C.c_int32),
                 ("stream", C.c_void_p), ("reserved", C.c_int32 * 8)]
 
+
+class Generator(C.Structure):
+    """tbmd_generator: the reference particlegenerator's parameters."""
+    _fields_ = [("kind", C.c_int32), ("n", C.c_int64), ("box", C.c_double * 3), ("corner", C.c_double * 3),
+                ("velocity", C.c_double * 3), ("mass", C.c_double), ("seed0", C.c_uint32), ("seed1", C.c_uint32),
+                ("n_clusters", C.c_int32), ("mean", C.c_double), ("stddev", C.c_double), ("csv_digits", C.c_int32),
+                ("reserved", C.c_int32 * 7)]
+
+
+GENERATORS = {"uniform": 0, "clusteredgauss": 1}
 
 _lib = None
 
@@ -78,6 +89,8 @@ def load():
         "tbmd_set_profiling": (C.c_int, [vp, i32]),
         "tbmd_phase_times": (i32, [vp, d, pu64, pu64, i32]),
         "tbmd_nata_forces_noalloc": (C.c_int, [i64, vp, vp, vp, C.c_double, i32, vp, vp, vp, vp]),
+        "tbmd_generator_init": (None, [C.POINTER(Generator)]),
+        "tbmd_generate_particles": (C.c_int, [vp, C.POINTER(Generator)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -156,6 +169,22 @@ class Context:
             idp = ids.ctypes.data_as(C.POINTER(C.c_int32))
         self._check(self._lib.tbmd_set_particles(self._h, n, idp, *[dptr(a) for a in arrs]))
         self.n = n
+
+    def generate(self, kind="uniform", n=0, box=(10.0, 10.0, 10.0), corner=(0.0, 0.0, 0.0), velocity=(0.0, 0.0, 0.0),
+                 mass=1.0, seed0=926762934, seed1=89347587, n_clusters=1, mean=0.0, stddev=1.0, csv_digits=6):
+        """Generate the reference particlegenerator's particles on the device and load them
+        (tbmd_generate_particles).  Returns the number of particles."""
+        g = Generator()
+        self._lib.tbmd_generator_init(C.byref(g))
+        g.kind = GENERATORS[kind] if isinstance(kind, str) else int(kind)
+        g.n = int(n)
+        for k in range(3):
+            g.box[k], g.corner[k], g.velocity[k] = float(box[k]), float(corner[k]), float(velocity[k])
+        g.mass, g.seed0, g.seed1 = float(mass), int(seed0) & 0xFFFFFFFF, int(seed1) & 0xFFFFFFFF
+        g.n_clusters, g.mean, g.stddev, g.csv_digits = int(n_clusters), float(mean), float(stddev), int(csv_digits)
+        self._check(self._lib.tbmd_generate_particles(self._h, C.byref(g)))
+        self.n = int(self._lib.tbmd_num_particles(self._h))
+        return self.n
 
     def set_state(self, st: dict):
         self.set_particles(st["x"], st["y"], st["z"], st.get("vx"), st.get("vy"), st.get("vz"), st.get("ax"),

@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstddef>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -64,6 +65,7 @@ struct tbmd_ctx {
     double *s[13] = {};
     DevBuf snapshot;  // copy of x..az taken before a multi-step run (capacity retry)
     DevBuf staging;   // tbmd_set_particles: incoming arrays and their check result
+    DevBuf gen_buf;   // tbmd_generate_particles: generator words, cluster centres, scan scratch
 
     // scalars: energy, count_cur, step counter, per-step counts
     DevBuf scalars;
@@ -624,7 +626,7 @@ void tbmd_destroy(tbmd_ctx *ctx)
     for (DevBuf *b : {&ctx->state, &ctx->snapshot, &ctx->scalars, &ctx->step_counts, &ctx->prefix, &ctx->partial,
                       &ctx->cell_n, &ctx->cell_c, &ctx->nbr_buf, &ctx->dirs, &ctx->hvp, &ctx->gset_single,
                       &ctx->sweep_sys, &ctx->bpos, &ctx->bout, &ctx->bsys, &ctx->bprefix, &ctx->ncell_tab,
-                      &ctx->staging, &ctx->long_buf})
+                      &ctx->staging, &ctx->long_buf, &ctx->gen_buf})
         b->release();
     if (ctx->hpin) cudaFreeHost(ctx->hpin);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -634,26 +636,14 @@ void tbmd_destroy(tbmd_ctx *ctx)
 int64_t tbmd_num_particles(const tbmd_ctx *ctx) { return ctx ? ctx->n : 0; }
 uint64_t tbmd_kernel_launches(const tbmd_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
-tbmd_status tbmd_set_particles(tbmd_ctx *ctx, int64_t n, const int32_t *id, const double *x, const double *y,
-                               const double *z, const double *vx, const double *vy, const double *vz,
-                               const double *ax, const double *ay, const double *az, const double *m)
+// The incoming particle arrays are in ctx->staging (x y z vx vy vz ax ay az m, n each): check them on
+// the device (non-finite values, masses <= 0, extremes of x, y, z for the domain) and make them the
+// context's state.  The state is untouched when the check fails.
+static tbmd_status commit_staging(tbmd_ctx *ctx, int64_t n, const int32_t *id)
 {
-    if (!ctx) return TBMD_INVALID_ARG;
-    if (n < 1 || n > (int64_t)INT32_MAX / 2) return fail(ctx, TBMD_INVALID_ARG, "n = %lld out of range", (long long)n);
-    const double *src[10] = {x, y, z, vx, vy, vz, ax, ay, az, m};
-    for (int k = 0; k < 10; ++k)
-        if (!src[k]) return fail(ctx, TBMD_INVALID_ARG, "null particle array %d", k);
-    tbmd_status st = check_device(ctx);
-    if (st != TBMD_OK) return st;
-    CK(cudaStreamSynchronize(ctx->stream));
-    // The arrays go to a staging buffer and are checked there on the device (non-finite values,
-    // masses <= 0, extremes of x, y, z for the domain); the state is replaced only if they pass.
     const size_t arr_bytes = sizeof(double) * 10 * (size_t)n;
-    CK(ctx->staging.ensure(arr_bytes + sizeof(ValidateResult) + 256));
     double *stg = ctx->staging.as<double>();
     ValidateResult *vr = (ValidateResult *)(ctx->staging.as<char>() + arr_bytes);
-    for (int k = 0; k < 10; ++k)
-        CK(cudaMemcpyAsync(stg + (size_t)k * n, src[k], sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
     CK(launch_validate(n, stg, vr, sms * 4, ctx->stream));
@@ -691,6 +681,130 @@ tbmd_status tbmd_set_particles(tbmd_ctx *ctx, int64_t n, const int32_t *id, cons
         ctx->cap = 0;
     }
     return TBMD_OK;
+}
+
+static cudaError_t ensure_staging(tbmd_ctx *ctx, int64_t n)
+{
+    return ctx->staging.ensure(sizeof(double) * 10 * (size_t)n + sizeof(ValidateResult) + 256);
+}
+
+tbmd_status tbmd_set_particles(tbmd_ctx *ctx, int64_t n, const int32_t *id, const double *x, const double *y,
+                               const double *z, const double *vx, const double *vy, const double *vz,
+                               const double *ax, const double *ay, const double *az, const double *m)
+{
+    if (!ctx) return TBMD_INVALID_ARG;
+    if (n < 1 || n > (int64_t)INT32_MAX / 2) return fail(ctx, TBMD_INVALID_ARG, "n = %lld out of range", (long long)n);
+    const double *src[10] = {x, y, z, vx, vy, vz, ax, ay, az, m};
+    for (int k = 0; k < 10; ++k)
+        if (!src[k]) return fail(ctx, TBMD_INVALID_ARG, "null particle array %d", k);
+    tbmd_status st = check_device(ctx);
+    if (st != TBMD_OK) return st;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(ensure_staging(ctx, n));
+    double *stg = ctx->staging.as<double>();
+    for (int k = 0; k < 10; ++k)
+        CK(cudaMemcpyAsync(stg + (size_t)k * n, src[k], sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    return commit_staging(ctx, n, id);
+}
+
+void tbmd_generator_init(tbmd_generator *g)
+{
+    if (!g) return;
+    std::memset(g, 0, sizeof *g);
+    g->kind = TBMD_GEN_UNIFORM;
+    for (int d = 0; d < 3; ++d) g->box[d] = 10.0;
+    g->mass = 1.0;
+    g->seed0 = 926762934u;
+    g->seed1 = 89347587u;
+    g->n_clusters = 1;
+    g->mean = 0.0;
+    g->stddev = 1.0;
+    g->csv_digits = 6;
+}
+
+// printf("%.6g") read back by strtod, on the host (the constant columns)
+static double csv6(double v)
+{
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%.6g", v);
+    return std::strtod(buf, nullptr);
+}
+
+tbmd_status tbmd_generate_particles(tbmd_ctx *ctx, const tbmd_generator *g)
+{
+    if (!ctx) return TBMD_INVALID_ARG;
+    if (!g) return fail(ctx, TBMD_INVALID_ARG, "null generator");
+    if (g->kind != TBMD_GEN_UNIFORM && g->kind != TBMD_GEN_CLUSTERED_GAUSS)
+        return fail(ctx, TBMD_INVALID_ARG, "unknown generator kind %d", g->kind);
+    if (g->csv_digits != 0 && g->csv_digits != 6) return fail(ctx, TBMD_INVALID_ARG, "csv_digits must be 0 or 6");
+    for (int d = 0; d < 3; ++d)
+        if (!std::isfinite(g->box[d]) || !std::isfinite(g->corner[d]) || !std::isfinite(g->velocity[d]))
+            return fail(ctx, TBMD_INVALID_ARG, "box, corner and velocity must be finite");
+    if (!(g->mass > 0) || !std::isfinite(g->mass)) return fail(ctx, TBMD_INVALID_ARG, "mass must be positive");
+    const bool clustered = g->kind == TBMD_GEN_CLUSTERED_GAUSS;
+    if (clustered && (g->n_clusters < 1 || !std::isfinite(g->mean) || !std::isfinite(g->stddev)))
+        return fail(ctx, TBMD_INVALID_ARG, "clustered generator needs n_clusters >= 1 and a finite mean/stddev");
+    const int64_t per = clustered ? g->n / g->n_clusters : 1;
+    const int64_t n = clustered ? per * g->n_clusters : g->n;  // ClusteredGaussGenerator.cpp:40
+    if (n < 1 || n > (int64_t)INT32_MAX / 2)
+        return fail(ctx, TBMD_INVALID_ARG, "n = %lld out of range", (long long)n);
+    tbmd_status st = check_device(ctx);
+    if (st != TBMD_OK) return st;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(ensure_staging(ctx, n));
+    double *stg = ctx->staging.as<double>();
+    double *X = stg, *Y = stg + n, *Z = stg + 2 * n;
+    cudaStream_t sm = ctx->stream;
+    if (!clustered) {
+        CK(ctx->gen_buf.ensure(sizeof(uint32_t) * 6 * (size_t)n));
+        CK(launch_mt19937(g->seed0, 6 * n, ctx->gen_buf.as<uint32_t>(), sm));
+        CK(launch_uniform_positions(n, ctx->gen_buf.as<uint32_t>(), g->corner, g->box, X, Y, Z, sm));
+        ctx->launches += 2;
+    } else {
+        // cluster centres: uniform draws from mt19937(seed1); then the Gaussian offsets in passes
+        const int64_t ncl = g->n_clusters;
+        const int64_t attempts = polar_attempts_per_pass();
+        const size_t cen_bytes = ((sizeof(double) * 3 * ncl + 255) / 256) * 256;
+        const size_t word_bytes = ((sizeof(uint32_t) * 6 * ncl + 255) / 256) * 256;
+        CK(ctx->gen_buf.ensure(cen_bytes + word_bytes + polar_scratch_bytes(attempts)));
+        char *gb = ctx->gen_buf.as<char>();
+        double *cen = (double *)gb;
+        uint32_t *words = (uint32_t *)(gb + cen_bytes);
+        void *scratch = gb + cen_bytes + word_bytes;
+        CK(launch_mt19937(g->seed1, 6 * ncl, words, sm));
+        CK(launch_uniform_positions(ncl, words, g->corner, g->box, cen, cen + ncl, cen + 2 * ncl, sm));
+        ctx->launches += 2;
+        const double *centres[3] = {cen, cen + ncl, cen + 2 * ncl};
+        const uint64_t m31 = 2147483647ull, x0 = (uint64_t)g->seed0 % m31 == 0 ? 1 : (uint64_t)g->seed0 % m31;
+        const unsigned long long G = 3ull * (unsigned long long)((n + 1) / 2);  // particle pairs x 3 axes
+        unsigned long long done = 0, t0 = 0;
+        int passes = 0;
+        while (done < G) {
+            if (++passes > 64) return fail(ctx, TBMD_CUDA_ERROR, "Gaussian generator did not converge");
+            int64_t T = (int64_t)((double)(G - done) * 1.35) + 4096;
+            if (T > attempts) T = attempts;
+            unsigned long long end = 0;
+            CK(launch_polar_pass(x0, t0, T, done, G, n, per, centres, g->mean, g->stddev, X, Y, Z, scratch, &end,
+                                 sm));
+            CK(cudaStreamSynchronize(sm));
+            ctx->launches += 3;
+            done = end;
+            t0 += (unsigned long long)T;
+        }
+    }
+    if (g->csv_digits == 6) {
+        CK(launch_round_sig6(3 * n, stg, sm));
+        ctx->launches += 1;
+    }
+    const double vel[3] = {g->csv_digits == 6 ? csv6(g->velocity[0]) : g->velocity[0],
+                           g->csv_digits == 6 ? csv6(g->velocity[1]) : g->velocity[1],
+                           g->csv_digits == 6 ? csv6(g->velocity[2]) : g->velocity[2]};
+    const double mass = g->csv_digits == 6 ? csv6(g->mass) : g->mass;
+    for (int d = 0; d < 3; ++d) CK(launch_fill(n, vel[d], stg + (3 + d) * n, sm));
+    CK(cudaMemsetAsync(stg + 6 * n, 0, sizeof(double) * 3 * n, sm));
+    CK(launch_fill(n, mass, stg + 9 * n, sm));
+    ctx->launches += 4;
+    return commit_staging(ctx, n, nullptr);
 }
 
 tbmd_status tbmd_set_domain(tbmd_ctx *ctx, const double *L, const double *lo)

@@ -310,6 +310,21 @@ struct ValidateResult {
 cudaError_t launch_validate(int64_t n, const double *arrays, ValidateResult *res, int grid, cudaStream_t st);
 double key_to_double(unsigned long long key);
 
+// Particle generation identical to the reference's particlegenerator (tbmd_gen.cu).
+cudaError_t launch_mt19937(uint32_t seed, int64_t nwords, uint32_t *out, cudaStream_t st);
+cudaError_t launch_uniform_positions(int64_t n, const uint32_t *words, const double corner[3], const double box[3],
+                                     double *x, double *y, double *z, cudaStream_t st);
+size_t polar_scratch_bytes(int64_t attempts);
+int64_t polar_attempts_per_pass();
+// One pass of T polar-method attempts from attempt t0 (generation indices from g0 on); writes the
+// particles of generations < G and the generation count after the pass to *accepted_end (host).
+cudaError_t launch_polar_pass(uint64_t x0, uint64_t t0, int64_t T, unsigned long long g0, unsigned long long G,
+                              int64_t m, int64_t per, const double *const centres[3], double mean, double stddev,
+                              double *x, double *y, double *z, void *scratch, unsigned long long *accepted_end,
+                              cudaStream_t st);
+cudaError_t launch_round_sig6(int64_t n, double *a, cudaStream_t st);
+cudaError_t launch_fill(int64_t n, double v, double *a, cudaStream_t st);
+
 cudaError_t launch_record_count(unsigned long long *cur, unsigned long long *per_step, unsigned int *step,
                                 unsigned long long constant_count, cudaStream_t st);
 
