@@ -1171,12 +1171,13 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
             };
 
             if (mJ == 0) {
-                // pairs inside block A: circular diagonals
+                // pairs inside block A: circular diagonals; y = (lane + d) mod mA advances by one per
+                // diagonal (lanes past the block cycle through valid slots and are masked)
+                int y = own ? lane : 0;
                 for (int d = 1; 2 * d <= mA; ++d) {
-                    int y = lane + d;
-                    if (y >= mA) y -= mA;
+                    y = y + 1 == mA ? 0 : y + 1;
                     const bool act = own && (2 * d < mA || lane < d);
-                    const int b = A0 + (y < mA ? y : 0);  // lanes past the block read a valid slot, masked
+                    const int b = A0 + y;
                     const PGrad<S> gb = pair(act, b);
                     if (act) pgrad_add(W.gr[b], gb, u);
                     __syncwarp();
