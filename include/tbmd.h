@@ -184,7 +184,8 @@ const char *tbmd_tuning(const tbmd_ctx *ctx);
  * events between phases on the context stream; times accumulate until tbmd_set_profiling is
  * called again.  Phases, in this order: 0 predictor, 1 cell build (counting sort), 2 neighbour
  * lists, 3 triplet forces (the P3BCA kernel or the NATA/AUTA sweep), 4 update (incl. unsort and
- * count bookkeeping).  tbmd_phase_times fills up to max entries of ms (milliseconds), calls (phase
+ * count bookkeeping).  In a P3BCA step the predictor is fused into the cell build and reported
+ * there (phase 0 stays empty).  tbmd_phase_times fills up to max entries of ms (milliseconds), calls (phase
  * executions) and launches (kernels launched in the phase) and returns the number of phases. */
 tbmd_status tbmd_set_profiling(tbmd_ctx *ctx, int32_t on);
 int32_t tbmd_phase_times(const tbmd_ctx *ctx, double *ms, uint64_t *calls, uint64_t *launches, int32_t max);

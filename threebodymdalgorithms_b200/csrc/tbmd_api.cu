@@ -438,10 +438,8 @@ static tbmd_status enqueue_forces(tbmd_ctx *ctx, int64_t n, Pos pos, Out out, bo
         phase_mark(ctx, st, PH_NEIGHBORS, *nl);
         CK(launch_neighbors(n, ctx->grid, ctx->gset, ctx->ncell_tab.as<int32_t>(), ctx->max_stage, cb, st));
         *nl += 1;
-        for (int k = 0; k < 3; ++k) {
-            CK(cudaMemsetAsync(cb.fs[k], 0, sizeof(double) * n, st));
-            if (dual) CK(cudaMemsetAsync(cb.hs[k], 0, sizeof(double) * n, st));
-        }
+        CK(cudaMemsetAsync(cb.fs[0], 0, sizeof(double) * 3 * n, st));  // fs[0..2] are adjacent
+        if (dual) CK(cudaMemsetAsync(cb.hs[0], 0, sizeof(double) * 3 * n, st));
         phase_mark(ctx, st, PH_TRIPLETS, *nl);
         CK(launch_p3bca(mx, dual, energy != nullptr, n, ctx->grid, ctx->gset, cb, nu, energy, count, ctx->plan, st));
         *nl += 1;
@@ -490,6 +488,26 @@ static tbmd_status enqueue_step(tbmd_ctx *ctx, cudaStream_t st, int *nl)
 {
     const int64_t n = ctx->n;
     double **s = ctx->s;
+    if (is_p3bca_cut(ctx)) {
+        // predictor + cell build, lists, triplets, then unsort + update + count in one kernel
+        CellBufs &cb = ctx->cb;
+        phase_mark(ctx, st, PH_CELLS, *nl);  // the predictor runs inside the cell build
+        CK(launch_step_cells(n, s, ctx->cfg.dt, ctx->grid, cb, st, nl));
+        phase_mark(ctx, st, PH_NEIGHBORS, *nl);
+        CK(launch_neighbors(n, ctx->grid, ctx->gset, ctx->ncell_tab.as<int32_t>(), ctx->max_stage, cb, st));
+        *nl += 1;
+        CK(cudaMemsetAsync(cb.fs[0], 0, sizeof(double) * 3 * n, st));  // fs[0..2] are adjacent
+        phase_mark(ctx, st, PH_TRIPLETS, *nl);
+        CK(launch_p3bca(mixed(ctx), false, false, n, ctx->grid, ctx->gset, cb, ctx->cfg.nu, nullptr, count_ptr(ctx),
+                        ctx->plan, st));
+        *nl += 1;
+        phase_mark(ctx, st, PH_UPDATE, *nl);
+        CK(launch_unsort_update(n, cb, s, ctx->cfg.dt, ctx->cfg.g, count_ptr(ctx),
+                                ctx->step_counts.as<unsigned long long>(), step_ptr(ctx), st));
+        *nl += 2;
+        phase_mark(ctx, st, PH_END, *nl);
+        return TBMD_OK;
+    }
     phase_mark(ctx, st, PH_PREDICTOR, *nl);
     CK(launch_predictor(n, s[0], s[1], s[2], s[3], s[4], s[5], s[6], ctx->cfg.dt, st));
     *nl += 1;
@@ -1380,10 +1398,8 @@ static tbmd_status batch_eval(tbmd_ctx *ctx, int32_t nsys, const int64_t *offset
             CellBufs &cb = ctx->cb;
             CK(launch_cell_build(N, pos, ctx->grid, ctx->gset, cb, dual, sm, &nl));
             CK(launch_neighbors(N, ctx->grid, ctx->gset, ctx->ncell_tab.as<int32_t>(), ctx->max_stage, cb, sm));
-            for (int k = 0; k < 3; ++k) {
-                CK(cudaMemsetAsync(cb.fs[k], 0, sizeof(double) * N, sm));
-                if (dual) CK(cudaMemsetAsync(cb.hs[k], 0, sizeof(double) * N, sm));
-            }
+            CK(cudaMemsetAsync(cb.fs[0], 0, sizeof(double) * 3 * N, sm));  // fs[0..2] are adjacent
+            if (dual) CK(cudaMemsetAsync(cb.hs[0], 0, sizeof(double) * 3 * N, sm));
             CK(launch_p3bca(mx, dual, true, N, ctx->grid, ctx->gset, cb, nu, E, CNT, ctx->plan, sm));
             CK(launch_unsort(N, cb, out, dual, sm));
             nl += 3 + (dual ? 1 : 0);

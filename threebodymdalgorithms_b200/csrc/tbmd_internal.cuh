@@ -273,6 +273,13 @@ struct CellBufs {
 // For a GridSet, g is the first system's grid with ncells = total cells over all systems.
 cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, const GridSet &set, CellBufs &cb, bool with_dir,
                               cudaStream_t st, int *launches);
+// The step of one system: predictor fused into the cell build; unsort, then the update fused with
+// the step's count record (st13: the 13 state arrays x y z vx vy vz ax ay az m fx fy fz).
+cudaError_t launch_step_cells(int64_t n, double *const st13[13], double dt, const Grid &g, CellBufs &cb,
+                              cudaStream_t st, int *launches);
+cudaError_t launch_unsort_update(int64_t n, const CellBufs &cb, double *const st13[13], double dt, const double g3[3],
+                                 unsigned long long *cur, unsigned long long *per_step, unsigned int *step,
+                                 cudaStream_t st);
 cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, const int32_t *nbr_cells, int max_stage,
                              CellBufs &cb, cudaStream_t st);
 int neighbor_stage_cap(const Grid &g, int64_t n);

@@ -569,14 +569,124 @@ cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, const GridSet &
 {
     const unsigned nb = (unsigned)((n + 255) / 256);
     cudaError_t e;
-    if ((e = cudaMemsetAsync(cb.cell_count, 0, sizeof(int32_t) * g.ncells, st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(cb.cell_fill, 0, sizeof(int32_t) * g.ncells, st)) != cudaSuccess) return e;
+    // cell_count and cell_fill are adjacent (cell_fill = cell_count + ncells): one memset
+    if ((e = cudaMemsetAsync(cb.cell_count, 0, sizeof(int32_t) * 2 * g.ncells, st)) != cudaSuccess) return e;
     k_cell_assign<<<nb, 256, 0, st>>>(n, pos.x, pos.y, pos.z, g, set, cb.cell_of, cb.cell_count);
     k_cell_scan<<<1, 1024, 0, st>>>(g.ncells, cb.cell_count, cb.cell_start);
     k_cell_scatter<<<nb, 256, 0, st>>>(n, cb.cell_of, cb.cell_start, cb.cell_fill, cb.sorted);
     k_gather<<<nb, 256, 0, st>>>(n, cb.sorted, pos, g, set, cb.xs, cb.ys, cb.zs, cb.qhi, cb.qlo,
                                  with_dir ? cb.dxs : nullptr, with_dir ? cb.dys : nullptr, with_dir ? cb.dzs : nullptr);
     if (launches) *launches += 4;
+    return cudaGetLastError();
+}
+
+// The Simulation step of one system fuses the integrator into the cell build and the unsort:
+//   k_predict_assign  predictor (structs.hpp:40-55) and the cell of the moved particle
+//   k_scatter_gather  slot in the counting sort, and the particle's positions written to that slot
+//   k_update_record   update (structs.hpp:57-99) and the step's count record, after k_unsort
+// The arithmetic per particle is that of k_predictor / k_cell_assign / k_gather / k_update, so the
+// results are identical; the step needs fewer launches and passes over memory.
+__global__ void k_predict_assign(int64_t n, double *x, double *y, double *z, const double *vx, const double *vy,
+                                 const double *vz, const double *ax, double dt, const __grid_constant__ Grid g,
+                                 int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double h = __dmul_rn(__dmul_rn(dt, dt), 0.5);
+    const double ah = __dmul_rn(ax[i], h);
+    const double px = __dadd_rn(__dadd_rn(x[i], __dmul_rn(vx[i], dt)), ah);
+    const double py = __dadd_rn(__dadd_rn(y[i], __dmul_rn(vy[i], dt)), ah);
+    const double pz = __dadd_rn(__dadd_rn(z[i], __dmul_rn(vz[i], dt)), ah);
+    x[i] = px;
+    y[i] = py;
+    z[i] = pz;
+    const int cx = cell_coord(px, g.lo[0], g.w[0], g.dims[0]);
+    const int cy = cell_coord(py, g.lo[1], g.w[1], g.dims[1]);
+    const int cz = cell_coord(pz, g.lo[2], g.w[2], g.dims[2]);
+    const int c = (cz * g.dims[1] + cy) * g.dims[0] + cx;
+    cell_of[i] = c;
+    atomicAdd(cell_count + c, 1);
+}
+
+__global__ void k_scatter_gather(int64_t n, const int32_t *__restrict__ cell_of, const int32_t *__restrict__ start,
+                                 int32_t *__restrict__ fill, int32_t *__restrict__ sorted,
+                                 const double *__restrict__ x, const double *__restrict__ y,
+                                 const double *__restrict__ z, const __grid_constant__ Grid g, double *xs, double *ys,
+                                 double *zs, float4 *qhi, float4 *qlo)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int c = cell_of[i];
+    const int slot = start[c] + atomicAdd(fill + c, 1);
+    sorted[slot] = (int32_t)i;
+    const double px = x[i], py = y[i], pz = z[i];
+    xs[slot] = px;
+    ys[slot] = py;
+    zs[slot] = pz;
+    float hx, hy, hz, lx, ly, lz;
+    split<float>(px - g.lo[0], 0.0, hx, lx);
+    split<float>(py - g.lo[1], 0.0, hy, ly);
+    split<float>(pz - g.lo[2], 0.0, hz, lz);
+    qhi[slot] = make_float4(hx, hy, hz, 0.f);
+    qlo[slot] = make_float4(lx, ly, lz, 0.f);
+}
+
+__global__ void k_unsort(int64_t n, const int32_t *__restrict__ sorted, const double *__restrict__ f0,
+                         const double *__restrict__ f1, const double *__restrict__ f2, double *o0, double *o1,
+                         double *o2);
+
+// update (structs.hpp:57-99, in input order, coalesced) and the step's triplet count record
+__global__ void k_update_record(int64_t n, double *vx, double *vy, double *vz, double *ax, double *ay, double *az,
+                                const double *__restrict__ fx, const double *__restrict__ fy,
+                                const double *__restrict__ fz, const double *__restrict__ m, double dt, double gx,
+                                double gy, double gz, unsigned long long *cur, unsigned long long *per_step,
+                                unsigned int *step)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {  // the step's triplet count (the triplet kernel has finished)
+        const unsigned int k = *step;
+        per_step[k] = *cur;
+        *step = k + 1;
+        *cur = 0ull;
+    }
+    if (i >= n) return;
+    const double h = __dmul_rn(dt, 0.5);
+    const double mi = m[i];
+    const double nx = __dsub_rn(gx, __ddiv_rn(fx[i], mi));
+    const double ny = __dsub_rn(gy, __ddiv_rn(fy[i], mi));
+    const double nz = __dsub_rn(gz, __ddiv_rn(fz[i], mi));
+    vx[i] = __dadd_rn(vx[i], __dmul_rn(nx, h));
+    vy[i] = __dadd_rn(vy[i], __dmul_rn(ny, h));
+    vz[i] = __dadd_rn(vz[i], __dmul_rn(nz, h));
+    ax[i] = nx;
+    ay[i] = ny;
+    az[i] = nz;
+}
+
+cudaError_t launch_step_cells(int64_t n, double *const st13[13], double dt, const Grid &g, CellBufs &cb,
+                              cudaStream_t st, int *launches)
+{
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(cb.cell_count, 0, sizeof(int32_t) * 2 * g.ncells, st)) != cudaSuccess) return e;
+    k_predict_assign<<<nb, 256, 0, st>>>(n, st13[0], st13[1], st13[2], st13[3], st13[4], st13[5], st13[6], dt, g,
+                                          cb.cell_of, cb.cell_count);
+    k_cell_scan<<<1, 1024, 0, st>>>(g.ncells, cb.cell_count, cb.cell_start);
+    k_scatter_gather<<<nb, 256, 0, st>>>(n, cb.cell_of, cb.cell_start, cb.cell_fill, cb.sorted, st13[0], st13[1],
+                                          st13[2], g, cb.xs, cb.ys, cb.zs, cb.qhi, cb.qlo);
+    if (launches) *launches += 3;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unsort_update(int64_t n, const CellBufs &cb, double *const st13[13], double dt, const double g3[3],
+                                 unsigned long long *cur, unsigned long long *per_step, unsigned int *step,
+                                 cudaStream_t st)
+{
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    // the scatter back to input order stays its own pass: the update then reads all arrays coalesced
+    k_unsort<<<nb, 256, 0, st>>>(n, cb.sorted, cb.fs[0], cb.fs[1], cb.fs[2], st13[10], st13[11], st13[12]);
+    k_update_record<<<nb, 256, 0, st>>>(n, st13[3], st13[4], st13[5], st13[6], st13[7], st13[8], st13[10], st13[11],
+                                         st13[12], st13[9], dt, g3[0], g3[1], g3[2], cur, per_step, step);
     return cudaGetLastError();
 }
 
