@@ -146,3 +146,16 @@ def test_autograd_force_matching_step():
     f1, _ = at(x, 1.0)
     expect = 2 * (0.8 - 1.1) * (f1.detach() ** 2).sum().item()
     assert abs(nu.grad.item() - expect) <= 1e-4 * abs(expect)
+
+
+@pytest.mark.parametrize("algo,cutoff", [("auta", 0.0), ("p3bca", 2.0)])
+def test_batch_rejects_non_finite_positions(algo, cutoff):
+    from threebodymdalgorithms_b200 import TbmdError
+    systems = make_systems(3, 50, 120, seed=5)
+    offsets, cat = pack(systems)
+    cat["y"][offsets[1] + 7] = np.nan
+    ctx = Context(algo, "mixed", cutoff)
+    with pytest.raises(TbmdError) as e:
+        ctx.batch_forces(offsets, cat["x"], cat["y"], cat["z"])
+    assert e.value.status == 2
+    ctx.close()

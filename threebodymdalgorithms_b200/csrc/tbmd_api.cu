@@ -93,6 +93,7 @@ struct tbmd_ctx {
     DevBuf ncell_tab;     // neighbour-cell table of the cells being evaluated (27 per cell)
     Grid ncell_grid{};    // grid the single-system table was built for
     bool ncell_single = false;
+    std::vector<int32_t> ncell_batch_key;  // per-system dims the batched table was built for
     int max_stage = 256;  // neighbour staging capacity
     DevBuf cell_n, cell_c, nbr_buf;
     DevBuf long_buf;      // chunk-pair items of long half lists
@@ -109,6 +110,7 @@ struct tbmd_ctx {
 
     // batched evaluation (tbmd_batch_*): packed positions/directions/outputs and system tables
     DevBuf bpos, bout, bsys, bprefix;
+    DevBuf bext;  // batched input check: offsets, non-finite flag, per-system extremes
     void *hpin = nullptr;  // pinned host buffer of batched results
     size_t hpin_bytes = 0;
 
@@ -549,13 +551,6 @@ static tbmd_status check_device(tbmd_ctx *ctx)
     return TBMD_OK;
 }
 
-static bool finite3(const double *a, int64_t n)
-{
-    for (int64_t i = 0; i < n; ++i)
-        if (!std::isfinite(a[i])) return false;
-    return true;
-}
-
 // ---------------------------------------------------------------------------------------------
 // C ABI
 
@@ -644,7 +639,7 @@ void tbmd_destroy(tbmd_ctx *ctx)
     for (DevBuf *b : {&ctx->state, &ctx->snapshot, &ctx->scalars, &ctx->step_counts, &ctx->prefix, &ctx->partial,
                       &ctx->cell_n, &ctx->cell_c, &ctx->nbr_buf, &ctx->dirs, &ctx->hvp, &ctx->gset_single,
                       &ctx->sweep_sys, &ctx->bpos, &ctx->bout, &ctx->bsys, &ctx->bprefix, &ctx->ncell_tab,
-                      &ctx->staging, &ctx->long_buf, &ctx->gen_buf})
+                      &ctx->staging, &ctx->long_buf, &ctx->gen_buf, &ctx->bext})
         b->release();
     if (ctx->hpin) cudaFreeHost(ctx->hpin);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1301,8 +1296,6 @@ static tbmd_status batch_eval(tbmd_ctx *ctx, int32_t nsys, const int64_t *offset
         if (offsets[s + 1] < offsets[s]) return fail(ctx, TBMD_INVALID_ARG, "offsets must not decrease");
     const int64_t N = offsets[nsys];
     if (N < 1 || N > (int64_t)INT32_MAX / 2) return fail(ctx, TBMD_INVALID_ARG, "total n out of range");
-    for (const double *a : {x, y, z})
-        if (!finite3(a, N)) return fail(ctx, TBMD_BAD_INPUT, "non-finite position");
     const bool dual = gfx != nullptr;
     tbmd_status st = check_device(ctx);
     if (st != TBMD_OK) return st;
@@ -1325,6 +1318,24 @@ static tbmd_status batch_eval(tbmd_ctx *ctx, int32_t nsys, const int64_t *offset
         CK(cudaMemcpyAsync(P + 4 * N, gfy, sizeof(double) * N, cudaMemcpyHostToDevice, sm));
         CK(cudaMemcpyAsync(P + 5 * N, gfz, sizeof(double) * N, cudaMemcpyHostToDevice, sm));
     }
+    // positions checked and each system's extremes found on the device
+    const size_t ob = sizeof(int64_t) * (nsys + 1);
+    CK(ctx->bext.ensure(ob + 16 + sizeof(unsigned long long) * 6 * (size_t)nsys));
+    int64_t *d_off = ctx->bext.as<int64_t>();
+    unsigned int *d_bad = (unsigned int *)(ctx->bext.as<char>() + ob);
+    unsigned long long *d_keys = (unsigned long long *)(ctx->bext.as<char>() + ob + 16);
+    CK(cudaMemcpyAsync(d_off, offsets, ob, cudaMemcpyHostToDevice, sm));
+    {
+        int sms = 0;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+        CK(launch_batch_extents(N, P, P + N, P + 2 * N, d_off, nsys, d_bad, d_keys, sms * 4, sm));
+    }
+    std::vector<unsigned long long> keys(6 * (size_t)nsys);
+    unsigned int bad = 0;
+    CK(cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, sm));
+    CK(cudaMemcpyAsync(keys.data(), d_keys, sizeof(unsigned long long) * keys.size(), cudaMemcpyDeviceToHost, sm));
+    CK(cudaStreamSynchronize(sm));
+    if (bad) return fail(ctx, TBMD_BAD_INPUT, "non-finite position");
     CK(ctx->bout.ensure(sizeof(double) * (6 * (size_t)N + 2 * (size_t)nsys)));
     double *O = ctx->bout.as<double>();
     double *E = O + 6 * N;
@@ -1349,12 +1360,9 @@ static tbmd_status batch_eval(tbmd_ctx *ctx, int32_t nsys, const int64_t *offset
                     Ls[d] = box[3 * s + d];
                     los[d] = lo ? lo[3 * s + d] : 0.0;
                 } else {
-                    const double *p = d == 0 ? x : (d == 1 ? y : z);
-                    double mn = e > b ? p[b] : 0.0, mxv = mn;
-                    for (int64_t i = b; i < e; ++i) {
-                        mn = p[i] < mn ? p[i] : mn;
-                        mxv = p[i] > mxv ? p[i] : mxv;
-                    }
+                    // the reference's domain rule on this system's extremes (0 for an empty system)
+                    const double mn = e > b ? key_to_double(keys[6 * s + d]) : 0.0;
+                    const double mxv = e > b ? key_to_double(keys[6 * s + 3 + d]) : 0.0;
                     los[d] = mn - 0.0001;
                     Ls[d] = std::fabs((mxv + 0.0001) - los[d]);
                 }
@@ -1370,10 +1378,20 @@ static tbmd_status batch_eval(tbmd_ctx *ctx, int32_t nsys, const int64_t *offset
             const int sc = neighbor_stage_cap(grids[s], e - b);
             stage = sc > stage ? sc : stage;
         }
-        std::vector<int32_t> tab27((size_t)cell_off[nsys] * 27);
-        for (int s = 0; s < nsys; ++s) neighbor_cell_table(grids[s], cell_off[s], tab27.data());
-        CK(ctx->ncell_tab.ensure(sizeof(int32_t) * tab27.size()));
-        CK(cudaMemcpyAsync(ctx->ncell_tab.p, tab27.data(), sizeof(int32_t) * tab27.size(), cudaMemcpyHostToDevice, sm));
+        // the neighbour-cell table depends only on each system's cell counts per axis: rebuilt when
+        // they change (or after a single-system evaluation replaced it)
+        std::vector<int32_t> tkey(3 * (size_t)nsys);
+        for (int s = 0; s < nsys; ++s)
+            for (int d = 0; d < 3; ++d) tkey[3 * s + d] = grids[s].dims[d];
+        if (ctx->ncell_single || tkey != ctx->ncell_batch_key) {
+            std::vector<int32_t> tab27((size_t)cell_off[nsys] * 27);
+            for (int s = 0; s < nsys; ++s) neighbor_cell_table(grids[s], cell_off[s], tab27.data());
+            CK(ctx->ncell_tab.ensure(sizeof(int32_t) * tab27.size()));
+            CK(cudaMemcpyAsync(ctx->ncell_tab.p, tab27.data(), sizeof(int32_t) * tab27.size(), cudaMemcpyHostToDevice,
+                               sm));
+            CK(cudaStreamSynchronize(sm));  // tab27 lives on this stack frame
+            ctx->ncell_batch_key = tkey;
+        }
         ctx->ncell_single = false;  // the single-system table is rebuilt on the next single evaluation
         const size_t gbytes = sizeof(Grid) * nsys, obytes = sizeof(int64_t) * (nsys + 1);
         CK(ctx->bsys.ensure(gbytes + 2 * obytes + 64));

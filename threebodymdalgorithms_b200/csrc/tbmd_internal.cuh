@@ -316,6 +316,10 @@ struct ValidateResult {
 // arrays: x y z vx vy vz ax ay az m, n each, back to back
 cudaError_t launch_validate(int64_t n, const double *arrays, ValidateResult *res, int grid, cudaStream_t st);
 double key_to_double(unsigned long long key);
+// Batched input check: *bad = 1 on a non-finite position; keys[6 s + d] / keys[6 s + 3 + d] the order
+// keys of the minimum / maximum of coordinate d of system s.
+cudaError_t launch_batch_extents(int64_t n, const double *x, const double *y, const double *z, const int64_t *sys_off,
+                                 int nsys, unsigned int *bad, unsigned long long *keys, int grid, cudaStream_t st);
 
 // Particle generation identical to the reference's particlegenerator (tbmd_gen.cu).
 cudaError_t launch_mt19937(uint32_t seed, int64_t nwords, uint32_t *out, cudaStream_t st);

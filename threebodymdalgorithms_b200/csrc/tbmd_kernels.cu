@@ -1609,6 +1609,62 @@ cudaError_t launch_validate(int64_t n, const double *arrays, ValidateResult *res
     return cudaGetLastError();
 }
 
+// Per-system input check of a batch: non-finite positions (flag) and the extremes of x, y, z of each
+// system (order keys, keys[6 s + 0..2] minima, keys[6 s + 3..5] maxima; preset to ~0 / 0).
+__global__ void __launch_bounds__(256) k_batch_extents(int64_t n, const double *__restrict__ x,
+                                                       const double *__restrict__ y, const double *__restrict__ z,
+                                                       const int64_t *__restrict__ sys_off, int nsys,
+                                                       unsigned int *bad, unsigned long long *keys)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+        const int64_t i = i0 + threadIdx.x;
+        const bool in = i < n;
+        const double v[3] = {in ? x[i] : 0.0, in ? y[i] : 0.0, in ? z[i] : 0.0};
+        const int sys = in ? system_of(sys_off, nsys, i) : -1;
+        if (in && !(isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]))) atomicOr(bad, 1u);
+        // a warp whose lanes all belong to one system reduces first (systems are contiguous)
+        const int s0 = __shfl_sync(0xffffffffu, sys, 0);
+        if (__all_sync(0xffffffffu, sys == s0) && s0 >= 0) {
+            for (int d = 0; d < 3; ++d) {
+                unsigned long long lo = order_key(v[d]), hi = lo;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const unsigned long long a = __shfl_xor_sync(0xffffffffu, lo, o);
+                    const unsigned long long b = __shfl_xor_sync(0xffffffffu, hi, o);
+                    lo = a < lo ? a : lo;
+                    hi = b > hi ? b : hi;
+                }
+                if (lane == 0) {
+                    atomicMin(keys + 6 * s0 + d, lo);
+                    atomicMax(keys + 6 * s0 + 3 + d, hi);
+                }
+            }
+        } else if (in) {
+            for (int d = 0; d < 3; ++d) {
+                atomicMin(keys + 6 * sys + d, order_key(v[d]));
+                atomicMax(keys + 6 * sys + 3 + d, order_key(v[d]));
+            }
+        }
+    }
+}
+
+__global__ void k_init_extents(int nsys, unsigned int *bad, unsigned long long *keys)
+{
+    for (int k = threadIdx.x; k < 6 * nsys; k += blockDim.x) keys[k] = (k % 6) < 3 ? ~0ull : 0ull;
+    if (threadIdx.x == 0) *bad = 0u;
+}
+
+cudaError_t launch_batch_extents(int64_t n, const double *x, const double *y, const double *z, const int64_t *sys_off,
+                                 int nsys, unsigned int *bad, unsigned long long *keys, int grid, cudaStream_t st)
+{
+    k_init_extents<<<1, 256, 0, st>>>(nsys, bad, keys);
+    const int64_t need = (n + 255) / 256;
+    k_batch_extents<<<(unsigned)(need < grid ? need : grid), 256, 0, st>>>(n, x, y, z, sys_off, nsys, bad, keys);
+    return cudaGetLastError();
+}
+
 double key_to_double(unsigned long long key)
 {
     const unsigned long long b = (key >> 63) ? (key & 0x7fffffffffffffffull) : ~key;
