@@ -175,6 +175,29 @@ def test_c3_p3bca_full_size_vs_oracle(cutoff):
         ctx.close()
 
 
+def test_p3bca_one_million_particles_vs_oracle():
+    """N = 1,048,576 uniform at density 2.048 (box 80^3, 8x the C3 volume), cutoff 2: triplet
+    counts bit-exact against the oracle's cell list and forces within tolerance, in both
+    precisions; a step from zero velocity keeps the positions, so its count is the same."""
+    n = 1 << 20
+    side = generators.box_for_density(n)
+    gen = Context("auta")
+    gen.generate(kind="uniform", n=n, box=(side, side, side))
+    st = gen.get_state()
+    gen.close()
+    L, lo = O.domain(st["x"], st["y"], st["z"])
+    fx, fy, fz, c_ref = O.forces(st["x"], st["y"], st["z"], 1.0, 2.0, L, lo, nthreads=0)
+    ref = np.stack([fx, fy, fz], 1)
+    for prec, tol in (("fp64", FP64_TOL), ("mixed", MIXED_FORCE_TOL)):
+        ctx = Context("p3bca", prec, 2.0, 0.001, (0.0, -9.81, 0.0))
+        ctx.set_state(st)
+        gfx, gfy, gfz, e, c = ctx.forces()
+        assert c == c_ref, (prec, c, c_ref)
+        assert rel_l2(np.stack([gfx, gfy, gfz], 1), ref) <= tol, prec
+        assert int(ctx.step(1)[0]) == c_ref
+        ctx.close()
+
+
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_p3bca_ten_steps_vs_oracle(prec):
     """Ten Simulation steps at N=16384 (density 2.048, c=2).  FP64 follows the reference's
