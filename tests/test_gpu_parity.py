@@ -198,6 +198,31 @@ def test_p3bca_one_million_particles_vs_oracle():
         ctx.close()
 
 
+def test_p3bca_particles_outside_the_domain():
+    """Positions are not wrapped into the box: particles moved one or more box lengths outside an
+    explicit domain are binned by wrapping, some into interior cells, and the cutoff test must
+    stay the reference's periodic formula on the raw coordinates."""
+    rng = np.random.default_rng(3)
+    n = 20000
+    side = generators.box_for_density(n)
+    st = generators.as_csv_values(generators.uniform(n, (side, side, side)))
+    L, lo = np.array([side] * 3), np.zeros(3)
+    moved = rng.choice(n, 300, replace=False)
+    shift = rng.integers(-3, 4, size=(300, 3)) * side + rng.uniform(-0.3, 0.3, size=(300, 3))
+    for d, k in enumerate("xyz"):
+        st[k][moved] += shift[:, d]
+    fx, fy, fz, c_ref = O.forces(st["x"], st["y"], st["z"], 1.0, 2.0, L, lo, nthreads=0)
+    ref = np.stack([fx, fy, fz], 1)
+    for prec, tol in (("fp64", FP64_TOL), ("mixed", MIXED_FORCE_TOL)):
+        ctx = Context("p3bca", prec, 2.0)
+        ctx.set_state(st)
+        ctx.set_domain(L, lo)
+        gfx, gfy, gfz, e, c = ctx.forces()
+        assert c == c_ref, (prec, c, c_ref)
+        assert rel_l2(np.stack([gfx, gfy, gfz], 1), ref) <= tol, prec
+        ctx.close()
+
+
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_p3bca_ten_steps_vs_oracle(prec):
     """Ten Simulation steps at N=16384 (density 2.048, c=2).  FP64 follows the reference's

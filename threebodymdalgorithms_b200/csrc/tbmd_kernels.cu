@@ -467,6 +467,18 @@ __device__ __forceinline__ int cell_coord(double x, double lo, double w, int nd)
     return (int)m;
 }
 
+// Cell coordinate as cell_coord, and whether it was reached by wrapping: the raw coordinate lies
+// outside the box (or is not a number).
+__device__ __forceinline__ int cell_coord_w(double x, double lo, double w, int nd, bool &outside)
+{
+    const double t = floor(__ddiv_rn(__dsub_rn(x, lo), w));
+    outside = outside || !(t >= 0.0 && t < (double)nd);
+    double m = fmod(t, (double)nd);
+    if (m < 0) m = __dadd_rn(m, (double)nd);
+    if (!(m >= 0.0 && m < (double)nd)) return 0;
+    return (int)m;
+}
+
 // Particle::GetSqrDistPeriodic (structs.hpp:106-115), evaluated in the reference's order.
 __device__ __forceinline__ double sqdist_periodic(double xa, double ya, double za, double xb, double yb, double zb,
                                                   const Grid &g)
@@ -485,18 +497,21 @@ __device__ __forceinline__ int system_of(const int64_t *sys_off, int nsys, int64
 
 __global__ void k_cell_assign(int64_t n, const double *__restrict__ x, const double *__restrict__ y,
                               const double *__restrict__ z, const __grid_constant__ Grid g, GridSet set,
-                              int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count)
+                              int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count,
+                              int32_t *__restrict__ cell_out)
 {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int sys = system_of(set.sys_off, set.nsys, i);
     const Grid &G = set.nsys > 1 ? set.grids[sys] : g;
-    int cx = cell_coord(x[i], G.lo[0], G.w[0], G.dims[0]);
-    int cy = cell_coord(y[i], G.lo[1], G.w[1], G.dims[1]);
-    int cz = cell_coord(z[i], G.lo[2], G.w[2], G.dims[2]);
+    bool out = false;
+    int cx = cell_coord_w(x[i], G.lo[0], G.w[0], G.dims[0], out);
+    int cy = cell_coord_w(y[i], G.lo[1], G.w[1], G.dims[1], out);
+    int cz = cell_coord_w(z[i], G.lo[2], G.w[2], G.dims[2], out);
     int c = (int)(set.nsys > 1 ? set.cell_off[sys] : 0) + (cz * G.dims[1] + cy) * G.dims[0] + cx;
     cell_of[i] = c;
     atomicAdd(cell_count + c, 1);
+    if (out) cell_out[c] = 1;
 }
 
 // Exclusive scan of cell counts (single block of 1024 threads, each owning a contiguous chunk).
@@ -569,9 +584,9 @@ cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, const GridSet &
 {
     const unsigned nb = (unsigned)((n + 255) / 256);
     cudaError_t e;
-    // cell_count and cell_fill are adjacent (cell_fill = cell_count + ncells): one memset
-    if ((e = cudaMemsetAsync(cb.cell_count, 0, sizeof(int32_t) * 2 * g.ncells, st)) != cudaSuccess) return e;
-    k_cell_assign<<<nb, 256, 0, st>>>(n, pos.x, pos.y, pos.z, g, set, cb.cell_of, cb.cell_count);
+    // cell_count, cell_fill and cell_out are adjacent: one memset
+    if ((e = cudaMemsetAsync(cb.cell_count, 0, sizeof(int32_t) * 3 * g.ncells, st)) != cudaSuccess) return e;
+    k_cell_assign<<<nb, 256, 0, st>>>(n, pos.x, pos.y, pos.z, g, set, cb.cell_of, cb.cell_count, cb.cell_out);
     k_cell_scan<<<1, 1024, 0, st>>>(g.ncells, cb.cell_count, cb.cell_start);
     k_cell_scatter<<<nb, 256, 0, st>>>(n, cb.cell_of, cb.cell_start, cb.cell_fill, cb.sorted);
     k_gather<<<nb, 256, 0, st>>>(n, cb.sorted, pos, g, set, cb.xs, cb.ys, cb.zs, cb.qhi, cb.qlo,
@@ -588,7 +603,8 @@ cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, const GridSet &
 // results are identical; the step needs fewer launches and passes over memory.
 __global__ void k_predict_assign(int64_t n, double *x, double *y, double *z, const double *vx, const double *vy,
                                  const double *vz, const double *ax, double dt, const __grid_constant__ Grid g,
-                                 int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count)
+                                 int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count,
+                                 int32_t *__restrict__ cell_out)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -600,12 +616,14 @@ __global__ void k_predict_assign(int64_t n, double *x, double *y, double *z, con
     x[i] = px;
     y[i] = py;
     z[i] = pz;
-    const int cx = cell_coord(px, g.lo[0], g.w[0], g.dims[0]);
-    const int cy = cell_coord(py, g.lo[1], g.w[1], g.dims[1]);
-    const int cz = cell_coord(pz, g.lo[2], g.w[2], g.dims[2]);
+    bool out = false;
+    const int cx = cell_coord_w(px, g.lo[0], g.w[0], g.dims[0], out);
+    const int cy = cell_coord_w(py, g.lo[1], g.w[1], g.dims[1], out);
+    const int cz = cell_coord_w(pz, g.lo[2], g.w[2], g.dims[2], out);
     const int c = (cz * g.dims[1] + cy) * g.dims[0] + cx;
     cell_of[i] = c;
     atomicAdd(cell_count + c, 1);
+    if (out) cell_out[c] = 1;
 }
 
 __global__ void k_scatter_gather(int64_t n, const int32_t *__restrict__ cell_of, const int32_t *__restrict__ start,
@@ -668,9 +686,9 @@ cudaError_t launch_step_cells(int64_t n, double *const st13[13], double dt, cons
 {
     const unsigned nb = (unsigned)((n + 255) / 256);
     cudaError_t e;
-    if ((e = cudaMemsetAsync(cb.cell_count, 0, sizeof(int32_t) * 2 * g.ncells, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(cb.cell_count, 0, sizeof(int32_t) * 3 * g.ncells, st)) != cudaSuccess) return e;
     k_predict_assign<<<nb, 256, 0, st>>>(n, st13[0], st13[1], st13[2], st13[3], st13[4], st13[5], st13[6], dt, g,
-                                          cb.cell_of, cb.cell_count);
+                                          cb.cell_of, cb.cell_count, cb.cell_out);
     k_cell_scan<<<1, 1024, 0, st>>>(g.ncells, cb.cell_count, cb.cell_start);
     k_scatter_gather<<<nb, 256, 0, st>>>(n, cb.cell_of, cb.cell_start, cb.cell_fill, cb.sorted, st13[0], st13[1],
                                           st13[2], g, cb.xs, cb.ys, cb.zs, cb.qhi, cb.qlo);
@@ -708,20 +726,25 @@ cudaError_t launch_unsort_update(int64_t n, const CellBufs &cb, double *const st
 // The test runs in FP32 on d = (hi_t - hi_s) + (lo_t - lo_s), which is within 2^-24 (|d| + L) of
 // the FP64 difference per component, inside the bound e = 16 eps32 (L + cutoff) of the guard band
 // (the triplet kernel's).  Outside the band around cutoff^2 the FP32 value decides; inside it the
-// exact FP64 test on the FP64 positions does, so the lists are exactly the reference's.  The
-// periodic form min(|d|, L - |d|) is always evaluated: positions are not wrapped into the box, so a
-// particle that drifted out of it sits in a cell at the other end with a raw offset near L.
+// exact FP64 test on the FP64 positions does, so the lists are exactly the reference's.
+// Positions are not wrapped into the box, so a particle that drifted out of it sits in a cell it
+// reached by wrapping, with a raw offset near a multiple of L; the cell build flags such cells
+// (cell_out).  A cell that is interior (at least 4 cells per axis, not on the boundary) and whose
+// candidate cells carry no flag has every coordinate inside the box and every candidate within
+// 2 cells <= L / 2 per axis: there the periodic form equals the raw distance and the hi parts alone
+// are accurate to 2^-24 L, so the cheaper test is used.  Elsewhere min(|d|, L - |d|) on hi + lo.
 constexpr int NB_THREADS = 128;
 constexpr size_t NB_STAGE_BYTES = 2 * sizeof(float4) + sizeof(int32_t);  // per staged candidate
 
-__global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant__ Grid g, GridSet set,
+__global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(const __grid_constant__ Grid g, GridSet set,
                                                           const int32_t *__restrict__ nbr_cells,
                                                           const float4 *__restrict__ qhi,
                                                           const float4 *__restrict__ qlo,
                                                           const double *__restrict__ xs,
                                                           const double *__restrict__ ys,
                                                           const double *__restrict__ zs,
-                                                          const int32_t *__restrict__ cell_start, int32_t *nbr,
+                                                          const int32_t *__restrict__ cell_start,
+                                                          const int32_t *__restrict__ cell_out, int32_t *nbr,
                                                           int32_t *nbr_count, int32_t *max_count, int cap,
                                                           int max_stage, unsigned long long *long_items,
                                                           unsigned int long_cap, unsigned int *long_count,
@@ -731,9 +754,10 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
     float4 *shi = (float4 *)smraw;
     float4 *slo = shi + max_stage;
     int32_t *st = (int32_t *)(slo + max_stage);
-    __shared__ int cstart[32], cpre[33];
+    __shared__ int cstart[32], cpre[33], raw_cell;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int NW = NB_THREADS / 32;
+    int warp_max = 0;  // longest list this warp produced (one atomic per warp at the end)
     for (int64_t c = blockIdx.x; c < g.ncells; c += gridDim.x) {
         const int b0 = cell_start[c], e0 = cell_start[c + 1];
         if (b0 == e0) continue;
@@ -745,6 +769,17 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
             const int nc = lane < 27 ? nbr_cells[c * 27 + lane] : -1;
             const int cs = nc >= 0 ? cell_start[nc] : 0;
             const int len = nc >= 0 ? cell_start[nc + 1] - cs : 0;
+            // raw test: an interior cell (at least 4 cells per axis, not on the boundary, so no
+            // candidate cell wraps) whose candidate cells hold only particles inside the box
+            const bool any_out = __any_sync(0xffffffffu, nc >= 0 && cell_out[nc] != 0);
+            if (lane == 0) {
+                const int64_t lc = c - (set.nsys > 1 ? set.cell_off[sys] : 0);
+                const int cx = (int)(lc % G.dims[0]), cy = (int)((lc / G.dims[0]) % G.dims[1]),
+                          cz = (int)(lc / ((int64_t)G.dims[0] * G.dims[1]));
+                const bool interior = G.dims[0] >= 4 && G.dims[1] >= 4 && G.dims[2] >= 4 && cx > 0 && cy > 0 &&
+                                      cz > 0 && cx < G.dims[0] - 1 && cy < G.dims[1] - 1 && cz < G.dims[2] - 1;
+                raw_cell = interior && !any_out;
+            }
             int incl = len;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -777,6 +812,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
             }
         }
         __syncthreads();
+        const bool raw = raw_cell != 0;
         for (int sl = warp; sl < e0 - b0; sl += NW) {
             const int s = b0 + sl;  // cell c comes first in the candidate order: q = sl
             const float4 oh = staged ? shi[sl] : qhi[s], ol = staged ? slo[sl] : qlo[s];
@@ -787,22 +823,29 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
                 bool pass = false;
                 int t = 0;
                 if (q < T) {
-                    float4 h, l;
+                    float4 h;
                     if (staged) {
                         t = st[q];
                         h = shi[q];
-                        l = slo[q];
                     } else {
                         const int k = entry_of(q);
                         t = cstart[k] + (q - cpre[k]);
                         h = qhi[t];
-                        l = qlo[t];
                     }
-                    const float dx = (h.x - oh.x) + (l.x - ol.x), dy = (h.y - oh.y) + (l.y - ol.y),
-                                dz = (h.z - oh.z) + (l.z - ol.z);
-                    const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
-                    const float mx = fminf(ax, Lx - ax), my = fminf(ay, Ly - ay), mz = fminf(az, Lz - az);
-                    const float d2 = fmaf(mx, mx, fmaf(my, my, mz * mz));
+                    float d2;
+                    if (raw) {
+                        // every coordinate lies in the box: the hi parts alone are within 2^-24 L, and
+                        // the periodic form is the raw distance (each axis under 2 cells <= L / 2)
+                        const float dx = h.x - oh.x, dy = h.y - oh.y, dz = h.z - oh.z;
+                        d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    } else {
+                        const float4 l = staged ? slo[q] : qlo[t];
+                        const float dx = (h.x - oh.x) + (l.x - ol.x), dy = (h.y - oh.y) + (l.y - ol.y),
+                                    dz = (h.z - oh.z) + (l.z - ol.z);
+                        const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
+                        const float mx = fminf(ax, Lx - ax), my = fminf(ay, Ly - ay), mz = fminf(az, Lz - az);
+                        d2 = fmaf(mx, mx, fmaf(my, my, mz * mz));
+                    }
                     pass = d2 <= sq_lo;
                     if (!pass && d2 <= sq_hi)
                         pass = sqdist_periodic(xs[s], ys[s], zs[s], xs[t], ys[t], zs[t], G) <= G.sqcut;
@@ -812,10 +855,8 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
                 if (pass && off < cap) dst[off] = t;
                 cnt += __popc(m);
             }
-            if (lane == 0) {
-                nbr_count[s] = cnt;
-                atomicMax(max_count, cnt);
-            }
+            if (lane == 0) nbr_count[s] = cnt;
+            warp_max = cnt > warp_max ? cnt : warp_max;
             // a list longer than one chunk: queue its chunk pairs (I <= J) for the triplet kernel
             const int M = cnt < cap ? cnt : cap;
             if (M > P3_CHUNK) {
@@ -840,15 +881,16 @@ __global__ void __launch_bounds__(NB_THREADS) k_neighbors(const __grid_constant_
         }
         __syncthreads();
     }
+    if (lane == 0 && warp_max > 0) atomicMax(max_count, warp_max);
 }
 
-// Staging capacity: 2.5 times the expected candidate count (14 of the 27 cells have id >= c on
+// Staging capacity: 1.6 times the expected candidate count (14 of the 27 cells have id >= c on
 // average), at least 256, at most 4096 (144 KiB).
 int neighbor_stage_cap(const Grid &g, int64_t n)
 {
     const double mean = (double)n / (double)g.ncells;
     const int cells = (g.dims[0] == 1 ? 1 : 3) * (g.dims[1] == 1 ? 1 : 3) * (g.dims[2] == 1 ? 1 : 3);
-    int want = (int)(2.5 * mean * (cells / 2 + 1)) + 128;
+    int want = (int)(1.6 * mean * (cells / 2 + 1)) + 128;
     want = (want + 31) / 32 * 32;
     return want < 256 ? 256 : (want > 4096 ? 4096 : want);
 }
@@ -892,7 +934,8 @@ cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, const
     cudaError_t e = cudaMemsetAsync(cb.long_count, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return e;
     k_neighbors<<<(unsigned)blocks, NB_THREADS, smem, st>>>(g, set, nbr_cells, cb.qhi, cb.qlo, cb.xs, cb.ys, cb.zs,
-                                                            cb.cell_start, cb.nbr, cb.nbr_count, cb.max_count, cb.cap,
+                                                            cb.cell_start, cb.cell_out, cb.nbr, cb.nbr_count,
+                                                            cb.max_count, cb.cap,
                                                             max_stage, cb.long_items, (unsigned int)cb.long_cap,
                                                             cb.long_count, cb.long_max);
     return cudaGetLastError();
