@@ -7,13 +7,17 @@
 //   c = |x_k - x_j|^2 = a + b - 2p,  q = u.(x_k - x_j) = p - a,  s = v.(x_k - x_j) = b - p
 //   D = p q s,  t = (a b c)^(-1/2)
 //   E = nu (1 + 3 cos g1 cos g2 cos g3) / (r1 r2 r3)^3 = nu t^3 (1 - 3 D t^2)
-// and the gradient of E(a, b, p) (c, q, s eliminated through c = a + b - 2p, q = p - a, s = b - p) is
-//   grad_j E = alpha u + gamma v,   grad_k E = beta v + gamma u,   grad_i E = -(grad_j E + grad_k E)
-// with alpha = 2 dE/da, beta = 2 dE/db, gamma = dE/dp:
+// and, with E a function of the three squared sides a, b, c, the gradient is written along the two
+// sides that meet at each particle (the reference's form, AxilrodTeller.cpp:83-93):
+//   grad_j E = alpha u + gamma w,   grad_k E = beta v - gamma w,   grad_i E = -(alpha u + beta v)
+// with w = x_k - x_j and alpha = 2 dE/da, beta = 2 dE/db, gamma = -2 dE/dc:
 //   m = -3 nu t^5,  B2 = m + 15 nu t^5 D t^2
-//   alpha = B2 b (a + c) - 2 m p s
-//   beta  = B2 a (b + c) + 2 m p q
+//   alpha = B2 b c + m (q s - p s - p q)
+//   beta  = B2 a c + m (q s + p s + p q)
 //   gamma = m (q s + p s - p q) - B2 a b
+// Writing grad_j in the basis (u, v) instead would need alpha + gamma and gamma separately, which
+// are large and nearly opposite when j and k are close and i is far: their rounding error is then
+// amplified by |u| / |w|.  Along the sides, no term cancels that way.
 // One reciprocal square root and no division per triplet.  The reference stores f = +grad E
 // (it subtracts -grad E into f), which these coefficients produce directly.
 #pragma once
@@ -109,33 +113,39 @@ __device__ __forceinline__ ATCoef<S> at_coef(S a, S b, S c, S p, S q, S s, S nu,
 {
     S m, B2;
     at_core<ENERGY>(a, b, c, p, q, s, nu, nu3, nu15, valid, e, m, B2);
-    S pq = p * q, ps = p * s;
-    S m2 = m + m;
+    S pq = p * q, ps = p * s, qs = q * s;
+    S x = qs + ps;
     ATCoef<S> r;
-    r.alpha = fma_(B2, b * (a + c), -(m2 * ps));
-    r.beta = fma_(B2, a * (b + c), m2 * pq);
-    r.gamma = fma_(m, fma_(q, s, ps - pq), -(B2 * (a * b)));
+    r.alpha = fma_(B2, b * c, m * (qs - (ps + pq)));
+    r.beta = fma_(B2, a * c, m * (x + pq));
+    r.gamma = fma_(m, x - pq, -(B2 * (a * b)));
     return r;
 }
 
-// Gradient on particle i alone, in the basis (u, w):  grad_i E = -(sigma u + tau w) with
-//   sigma = alpha + beta + 2 gamma = B2 c (a + b) + 2 m q s
-//   tau   = beta + gamma          = B2 a c + m (q s + p s + p q).
-// Summing alpha + gamma etc. numerically would cancel the large d/dc terms when i is far from a
-// close pair (j, k); these closed forms do not.
+// Gradient on particle i alone: grad_i E = -(alpha u + beta v) = -(sigma u + beta w)
+// = -(sigma v - alpha w) with sigma = alpha + beta in closed form,
+//   sigma = B2 c (a + b) + 2 m q s.
+// Each of the three forms cancels in one geometry: the side form when w is the shortest side (i far
+// from a close pair j, k: alpha ~ -beta, u ~ v), the (u, w) form when v is (beta w ~ -beta u), the
+// (v, w) form when u is.  The caller takes (u, w) when |u| <= |v| (ub) and (v, w) otherwise; the
+// side left out of the basis is then never the shortest, and no term exceeds the result by more
+// than the triangle's aspect ratio of 2.  kappa is the coefficient of w: beta, or -alpha.
 template <class S>
 struct ATSelf {
-    S sigma, tau;
+    S sigma, kappa;
 };
 template <bool ENERGY, class S>
-__device__ __forceinline__ ATSelf<S> at_self(S a, S b, S c, S p, S q, S s, S nu, S nu3, S nu15, bool valid, S &e)
+__device__ __forceinline__ ATSelf<S> at_self(S a, S b, S c, S p, S q, S s, S nu, S nu3, S nu15, bool valid, bool ub,
+                                             S &e)
 {
     S m, B2;
     at_core<ENERGY>(a, b, c, p, q, s, nu, nu3, nu15, valid, e, m, B2);
     S qs = q * s;
     ATSelf<S> r;
     r.sigma = fma_(B2, c * (a + b), (m + m) * qs);
-    r.tau = fma_(B2, a * c, m * fma_(p, q + s, qs));
+    // beta = B2 a c + m (q s + p (q + s)),  -alpha = B2 (-b) c + m (-q s + p (q + s))
+    const S x = ub ? a : -b, y = ub ? qs : -qs;
+    r.kappa = fma_(B2, x * c, m * fma_(p, q + s, y));
     return r;
 }
 

@@ -8,8 +8,8 @@
 //                k = tile + l and writes it with one FP64 atomic.  i's force is -(sum of the j- and
 //                k-side totals) by translation invariance, so it costs nothing per triplet.
 //   k_nata       NATA: all triplets seen from each particle i; only grad_i is accumulated (in the
-//                well-conditioned (u, w) form of at_self), no atomics; per-(i, j-block) partial
-//                sums are reduced in a fixed order (deterministic).
+//                well-conditioned (u, w) or (v, w) form of at_self), no atomics; per-(i, j-block)
+//                partial sums are reduced in a fixed order (deterministic).
 //   k_cell_*     P3BCA cell grid: wrap-and-bin (FP64, same arithmetic as the oracle), counting sort
 //                by cell, stable within a cell.
 //   k_neighbors  half neighbour lists (sorted index t > s) with the reference's exact FP64
@@ -99,12 +99,13 @@ __device__ __forceinline__ void edge(const Pos &p, int64_t j, double xi, double 
 }
 
 // The six scalars of a triplet from the edges u, v (hi/lo) of vertex i; c, q and s come from the
-// third edge itself, so no scalar is a difference of nearly equal numbers.
+// third edge w itself (returned for the gradients), so no scalar is a difference of nearly equal
+// numbers.
 template <bool ENERGY, class S>
 __device__ __forceinline__ ATCoef<S> triplet(V3<S> uh, V3<S> ul, S a, V3<S> vh, V3<S> vl, S b, S nu, S nu3, S nu15,
-                                             bool valid, S &e)
+                                             bool valid, S &e, V3<S> &w)
 {
-    const V3<S> w = third_edge(uh, ul, vh, vl);
+    w = third_edge(uh, ul, vh, vl);
     return at_coef<ENERGY>(a, b, dot3(w, w), dot3(uh, vh), dot3(uh, w), dot3(vh, w), nu, nu3, nu15, valid, e);
 }
 
@@ -121,6 +122,18 @@ __device__ __forceinline__ int find_block(const int64_t *prefix, int nblocks, in
     }
     return lo;
 }
+
+// value part as FP32 (comparisons that only choose between equivalent forms)
+template <class S>
+__device__ __forceinline__ float to_float(S v);
+template <>
+__device__ __forceinline__ float to_float<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ float to_float<double>(double v) { return (float)v; }
+template <>
+__device__ __forceinline__ float to_float<Dual<double>>(Dual<double> v) { return (float)v.v; }
+template <>
+__device__ __forceinline__ float to_float<Dual<float>>(Dual<float> v) { return v.v; }
 
 // ---------------------------------------------------------------------------------------------
 // AUTA sweep
@@ -196,7 +209,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
                 gv[r] = vzero<S>();
             }
             S bsum = szero<S>();
-            V3<S> gus = vzero<S>();
+            V3<S> gw = vzero<S>();
             S en = szero<S>();
 #pragma unroll 2
             for (int t = 0; t < 32; ++t) {
@@ -208,18 +221,19 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const bool valid = jv[r] && kidx > jj[r] && kidx < hi;
-                    const ATCoef<S> cf = triplet<ENERGY>(u[r], ul[r], aa[r], v, vl, e.b, nu, nu3, nu15, valid, en);
+                    V3<S> ec;  // third edge x_k - x_j
+                    const ATCoef<S> cf = triplet<ENERGY>(u[r], ul[r], aa[r], v, vl, e.b, nu, nu3, nu15, valid, en, ec);
                     al[r] = al[r] + cf.alpha;
-                    gv[r] = fma3(v, cf.gamma, gv[r]);
+                    gv[r] = fma3(ec, cf.gamma, gv[r]);
                     bsum = bsum + cf.beta;
-                    gus = fma3(u[r], cf.gamma, gus);
+                    gw = fma3(ec, -cf.gamma, gw);
                 }
                 const int src = (lane + 1) & 31;
                 bsum = shfl_idx(bsum, src);
-                gus = shfl_idx(gus, src);
+                gw = shfl_idx(gw, src);
             }
             // After the full rotation lane l holds the k-side sums of k = kt + l.
-            const V3<Acc> fk = widen(fma3(vk, bsum, gus));
+            const V3<Acc> fk = widen(fma3(vk, bsum, gw));
             if (kv) atomic_out(out, k, fk);
             fi = fi - fk;
 #pragma unroll
@@ -310,17 +324,24 @@ __global__ void __launch_bounds__(WARPS * 32) k_nata(int64_t n, Pos pos, double 
                 const V3<S> vl = e.lo();
                 const int64_t kidx = kt + t;
                 const bool kv = kidx < n && kidx != i;
+                S sv = szero<S>();  // sigma of the pairs taken in the (v, w) basis, for this k
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const bool valid = jv[r] && kv && kidx > jj[r];
                     S e_r = szero<S>();
                     const V3<S> w = third_edge(u[r], ul[r], v, vl);
+                    // basis (u, w) when |u| <= |v|, else (v, w): see at_self
+                    const bool ub = to_float(aa[r]) <= to_float(e.b);
                     const ATSelf<S> cf = at_self<ENERGY>(aa[r], e.b, dot3(w, w), dot3(u[r], v), dot3(u[r], w),
-                                                         dot3(v, w), nu, nu3, nu15, valid, e_r);
+                                                         dot3(v, w), nu, nu3, nu15, valid, ub, e_r);
                     if (ENERGY && i < jj[r]) en = en + e_r;
-                    A[r] = A[r] + cf.sigma;
-                    Tw = fma3(w, cf.tau, Tw);
+                    if (ub)
+                        A[r] = A[r] + cf.sigma;
+                    else
+                        sv = sv + cf.sigma;
+                    Tw = fma3(w, cf.kappa, Tw);
                 }
+                Tw = fma3(v, sv, Tw);
             }
             V3<S> gt = Tw;
 #pragma unroll
@@ -1010,54 +1031,56 @@ __device__ __forceinline__ void slot_add(Grad<S> &slot, V3<S> g)
 }
 
 // Factored accumulation.  A slot's edge e (hi part) is fixed during an item, so every gradient it
-// receives is (scalar) * e + (vector): as the own slot of a lane it gets alpha u + gamma v (e = u),
-// as a partner beta v + gamma u (e = v).  The mixed form keeps the scalar in the slot's spare fourth
-// float and the vector in x, y, z, and forms scalar * e + vector once, at the flush: 4 instead of
-// 9 FP32 operations per triplet and side.  The other forms accumulate the gradient itself.
+// receives is (scalar) * e + (vector): as the own slot of a lane it gets alpha u + gamma w (e = u),
+// as a partner beta v - gamma w (e = v), w the pair's third edge.  The mixed form keeps the scalar
+// in the slot's spare fourth float and the vector in x, y, z, and forms scalar * e + vector once,
+// at the flush: 4 instead of 9 FP32 operations per triplet and side.  The other forms accumulate
+// the gradient itself.
 template <class S>
 struct PGrad {  // a partner's share of one triplet
     V3<S> g;
 };
 template <>
 struct PGrad<float> {
-    float beta, gamma;
+    float beta, ngamma;  // beta and -gamma
+    V3<float> w;
 };
 template <class S>
-__device__ __forceinline__ PGrad<S> make_pgrad(const ATCoef<S> &cf, V3<S> u, V3<S> v)
+__device__ __forceinline__ PGrad<S> make_pgrad(const ATCoef<S> &cf, V3<S> v, V3<S> w)
 {
-    return PGrad<S>{fma3(v, cf.beta, u * cf.gamma)};
+    return PGrad<S>{fma3(v, cf.beta, w * (-cf.gamma))};
 }
 template <>
-__device__ __forceinline__ PGrad<float> make_pgrad<float>(const ATCoef<float> &cf, V3<float>, V3<float>)
+__device__ __forceinline__ PGrad<float> make_pgrad<float>(const ATCoef<float> &cf, V3<float>, V3<float> w)
 {
-    return PGrad<float>{cf.beta, cf.gamma};
+    return PGrad<float>{cf.beta, -cf.gamma, w};
 }
 template <class S>
-__device__ __forceinline__ void pgrad_add(Grad<S> &slot, const PGrad<S> &pg, V3<S>)
+__device__ __forceinline__ void pgrad_add(Grad<S> &slot, const PGrad<S> &pg)
 {
     slot_add(slot, pg.g);
 }
 template <>
-__device__ __forceinline__ void pgrad_add<float>(Grad<float> &slot, const PGrad<float> &pg, V3<float> u)
+__device__ __forceinline__ void pgrad_add<float>(Grad<float> &slot, const PGrad<float> &pg)
 {
     Grad<float> v = slot;
-    v.x = fmaf(pg.gamma, u.x, v.x);
-    v.y = fmaf(pg.gamma, u.y, v.y);
-    v.z = fmaf(pg.gamma, u.z, v.z);
+    v.x = fmaf(pg.ngamma, pg.w.x, v.x);
+    v.y = fmaf(pg.ngamma, pg.w.y, v.y);
+    v.z = fmaf(pg.ngamma, pg.w.z, v.z);
     v.w = v.w + pg.beta;
     slot = v;
 }
 // partner shares of all lanes for one common partner slot, added by lane 0
 template <class S>
-__device__ __forceinline__ void pgrad_add_warp(Grad<S> &slot, const PGrad<S> &pg, V3<S>, int lane)
+__device__ __forceinline__ void pgrad_add_warp(Grad<S> &slot, const PGrad<S> &pg, int lane)
 {
     const V3<S> g = warp_sum3s(pg.g);
     if (lane == 0) slot_add(slot, g);
 }
 template <>
-__device__ __forceinline__ void pgrad_add_warp<float>(Grad<float> &slot, const PGrad<float> &pg, V3<float> u, int lane)
+__device__ __forceinline__ void pgrad_add_warp<float>(Grad<float> &slot, const PGrad<float> &pg, int lane)
 {
-    V3<float> g = u * pg.gamma;
+    V3<float> g = pg.w * pg.ngamma;
     float beta = pg.beta;
 #pragma unroll
     for (int m = 16; m > 0; m >>= 1) {
@@ -1080,7 +1103,7 @@ template <class S>
 struct OwnAcc {
     V3<S> g;
     __device__ __forceinline__ void zero() { g = vzero<S>(); }
-    __device__ __forceinline__ void add(const ATCoef<S> &cf, V3<S> u, V3<S> v) { g = g + fma3(u, cf.alpha, v * cf.gamma); }
+    __device__ __forceinline__ void add(const ATCoef<S> &cf, V3<S> u, V3<S> w) { g = g + fma3(u, cf.alpha, w * cf.gamma); }
     __device__ __forceinline__ void merge(Grad<S> &slot) const { slot_add(slot, g); }
 };
 template <>
@@ -1092,10 +1115,10 @@ struct OwnAcc<float> {
         g = {0.f, 0.f, 0.f};
         alpha = 0.f;
     }
-    __device__ __forceinline__ void add(const ATCoef<float> &cf, V3<float>, V3<float> v)
+    __device__ __forceinline__ void add(const ATCoef<float> &cf, V3<float>, V3<float> w)
     {
         alpha += cf.alpha;
-        g = fma3(v, cf.gamma, g);
+        g = fma3(w, cf.gamma, g);
     }
     __device__ __forceinline__ void merge(Grad<float> &slot) const
     {
@@ -1132,16 +1155,6 @@ struct SlotLayout {
         (1 + nlo) * sizeof(Slot4<S>) + npos * sizeof(double) + sizeof(Grad<S>) + sizeof(int32_t);
 };
 
-template <class S>
-__device__ __forceinline__ float to_float(S v);
-template <>
-__device__ __forceinline__ float to_float<float>(float v) { return v; }
-template <>
-__device__ __forceinline__ float to_float<double>(double v) { return (float)v; }
-template <>
-__device__ __forceinline__ float to_float<Dual<double>>(Dual<double> v) { return (float)v.v; }
-template <>
-__device__ __forceinline__ float to_float<Dual<float>>(Dual<float> v) { return v.v; }
 
 template <class S>
 struct P3Warp {
@@ -1319,8 +1332,8 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
                 cnt += inside ? 1u : 0u;
                 const ATCoef<S> cf =
                     at_coef<ENERGY>(aa, pd.w, cww, dot3(u, v), dot3(u, wv), dot3(v, wv), nu, nu3, nu15, inside, en);
-                acc.add(cf, u, v);
-                return make_pgrad(cf, u, v);
+                acc.add(cf, u, wv);
+                return make_pgrad(cf, v, wv);
             };
 
             if (mJ == 0) {
@@ -1332,7 +1345,7 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
                     const bool act = own && (2 * d < mA || lane < d);
                     const int b = A0 + y;
                     const PGrad<S> gb = pair(act, b);
-                    if (act) pgrad_add(W.gr[b], gb, u);
+                    if (act) pgrad_add(W.gr[b], gb);
                     __syncwarp();
                 }
             }
@@ -1345,13 +1358,13 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
                         const bool act = own && y < mB;
                         const int b = B0 + (y < mB ? y : 0);
                         const PGrad<S> gb = pair(act, b);
-                        if (act) pgrad_add(W.gr[b], gb, u);
+                        if (act) pgrad_add(W.gr[b], gb);
                         __syncwarp();
                     }
                 } else {
                     for (int y = 0; y < mB; ++y) {
                         const int b = B0 + y;
-                        pgrad_add_warp(W.gr[b], pair(own, b), u, lane);
+                        pgrad_add_warp(W.gr[b], pair(own, b), lane);
                         __syncwarp();
                     }
                 }
