@@ -41,7 +41,8 @@ typedef enum {
     TBMD_CUDA_ERROR = 5,      /* a CUDA runtime call failed; see tbmd_last_error */
     TBMD_TIMEOUT = 6,         /* a bounded device-side wait gave up (the kernel returned early) */
     TBMD_NO_DEVICE = 7,       /* no CUDA device, or not an sm_100 device */
-    TBMD_TOO_LARGE = 8        /* n above the limit of an allocation-free entry point */
+    TBMD_TOO_LARGE = 8,       /* n above the limit of an allocation-free entry point */
+    TBMD_RANK_LAYOUT = 9      /* the reference's run on that many MPI ranks would stop (tbmd_rank_layout_of) */
 } tbmd_status;
 
 /* Same numbering as the reference's AlgorithmType (src/utility/enums.hpp). */
@@ -204,6 +205,41 @@ int32_t tbmd_phase_times(const tbmd_ctx *ctx, double *ms, uint64_t *calls, uint6
 #define TBMD_NOALLOC_MAX_N 4096
 tbmd_status tbmd_nata_forces_noalloc(int64_t n, const double *x, const double *y, const double *z, double nu,
                                      int32_t precision, double *fx, double *fy, double *fz, void *stream);
+
+/* Layout of the reference's run on P MPI ranks (host only, no device work).  Results do not depend
+ * on P: every rank layout evaluates each triplet once, and the GPU evaluates them all in one
+ * process.  What P decides in the reference is the process grid and whether the run starts, and
+ * this entry point restates that so that a caller (and tbmd_main -np P) stops where an
+ * `mpiexec -n P` run would, with the same message.
+ *
+ *   P3BCA: the process grid of main.cpp:546-551 (utility.cpp:96-107 over the tables of
+ *     utility/decompositions.hpp): naive = {P}; optimal = the factorisation of P into one to three
+ *     non-decreasing factors, each at least 3 unless it is P itself, with the smallest sum, the
+ *     lexicographically first among equal sums except P = 360 (6 x 6 x 10).  Tables end at
+ *     P = 1024; above it the grid is empty and the reference's CartTopology::Init reads past it
+ *     (CartTopology.cpp:10-12): TBMD_RANK_LAYOUT, with a message saying so.
+ *     Local cell width L / dims (RegularGridDecomposition.cpp:24-32), cutoff boxes per axis and
+ *     the cutoff-window check (P3BCA.cpp:29-70), shift steps per Simulation step (P3BCA.cpp:79-92).
+ *   NATA / AUTA: ring of P ranks; AtomDecomposition (AtomDecomposition.cpp:15-41) pads the first
+ *     P - n mod P ranks with one dummy particle each when n mod P != 0.
+ *
+ * L is the physical domain size (tbmd_cells returns it; P3BCA only, may be NULL otherwise).
+ * Returns TBMD_OK; TBMD_INVALID_ARG (bad algorithm, world_size < 1, n < 0, cutoff not finite,
+ * L not positive); TBMD_RANK_LAYOUT where the reference's run stops, with its stderr line in msg.
+ * msg may be NULL; otherwise up to msg_len bytes including the terminating 0 are written. */
+typedef struct tbmd_rank_layout {
+    int32_t world_size;
+    int32_t num_dims;            /* process-grid dimensions (1 for the NATA / AUTA ring) */
+    int32_t dims[3];             /* ranks per axis, 1 for unused axes */
+    int32_t cutoff_boxes[3];     /* P3BCA nCbX, nCbY, nCbZ */
+    int32_t shift_steps;         /* P3BCA CalculateInteractions rounds per Simulation step */
+    int32_t reserved;
+    double cell_size[3];         /* P3BCA local cell width per axis */
+    int64_t particles_per_rank;  /* NATA / AUTA particles per rank, dummies included */
+    int64_t dummies;             /* NATA / AUTA dummy particles over all ranks */
+} tbmd_rank_layout;
+tbmd_status tbmd_rank_layout_of(int32_t algorithm, int32_t world_size, int32_t optimal_decomposition, double cutoff,
+                                const double *L, int64_t n, tbmd_rank_layout *out, char *msg, int32_t msg_len);
 
 /* Wait for all work of the context's stream. */
 tbmd_status tbmd_sync(tbmd_ctx *ctx);

@@ -210,6 +210,28 @@ def reference_dump(csv: str, algo: str, mode: str = "sim", iters: int = 1, dt: f
     return st, np.array(counts, dtype=np.uint64), t
 
 
+def reference_layout(csv: str, algo: str, world_size: int, rank: int = 0, cutoff: float = 0.0,
+                     decomposition: str = "naive", timeout: float = 60.0):
+    """Run the reference's own set-up (Simulation::Init) for rank `rank` of `world_size` under the
+    stub MPI's layout mode (oracle/refstub/ref_layout.cpp).  Returns (exit status, stderr text,
+    the JSON it printed or None)."""
+    import json
+    cmd = [str(REF_DIR / "ref_layout"), "--algo", algo, "--csv", csv, "--cutoff", repr(float(cutoff)),
+           "--decomp", decomposition]
+    env = dict(os.environ, TBMD_STUB_WORLD_SIZE=str(world_size), TBMD_STUB_RANK=str(rank))
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout, env=env)
+    out = json.loads(r.stdout) if r.returncode == 0 and r.stdout.strip() else None
+    return r.returncode, r.stderr.strip(), out
+
+
+def reference_grid_tables() -> dict:
+    """The reference's process-grid tables (Utility::getDecomposition over utility/decompositions.hpp)
+    for P = 1..1030, as {"optimal": {P: grid}, "naive": {P: grid}} (an empty grid past the tables)."""
+    import json
+    r = subprocess.run([str(REF_DIR / "ref_layout"), "--tables"], capture_output=True, text=True, check=True)
+    return json.loads(r.stdout)
+
+
 def read_csv(path: str) -> dict:
     """Read a reference particle CSV (header row; ID, pX..pZ, vX..vZ, aX..aZ, m; extra columns ignored)."""
     a = np.loadtxt(path, delimiter=",", skiprows=1, ndmin=2)

@@ -15,6 +15,12 @@
  * Datatypes are small integers into a registry that records the extent, so that
  * MPI_Gather/Gatherv of the reference's Particle struct (structs.hpp:124-155)
  * copy the right number of bytes.
+ *
+ * Layout mode (the ref_layout driver): with TBMD_STUB_WORLD_SIZE=P and TBMD_STUB_RANK=r in the
+ * environment the world has P ranks and this process is rank r, so that the reference's set-up
+ * code (topologies, decompositions, Algorithm::Init) lays out a P-rank run for rank r.  Cartesian
+ * coordinates are row-major, as MPI defines them.  Set-up exchanges no message; every call that
+ * would move data between ranks aborts in this mode.  Without the variables the world is one rank.
  */
 #ifndef TBMD_REFSTUB_MPI_H
 #define TBMD_REFSTUB_MPI_H
@@ -92,12 +98,42 @@ static inline int tbmd_stub_unreachable(const char *what)
     return 1;
 }
 
+/* world size and own rank: {1, 0}, or the layout-mode environment */
+inline const int *tbmd_stub_world(void)
+{
+    static int w[2] = {-1, -1};
+    if (w[0] < 0) {
+        const char *ps = getenv("TBMD_STUB_WORLD_SIZE"), *rs = getenv("TBMD_STUB_RANK");
+        const int P = ps ? atoi(ps) : 1, r = rs ? atoi(rs) : 0;
+        if (P < 1 || r < 0 || r >= P) {
+            fprintf(stderr, "mpi stub: bad TBMD_STUB_WORLD_SIZE / TBMD_STUB_RANK\n");
+            abort();
+        }
+        w[0] = P;
+        w[1] = r;
+    }
+    return w;
+}
+/* the Cartesian grid of the last MPI_Cart_create: {ndims, d0, d1, d2} */
+inline int *tbmd_stub_cart(void)
+{
+    static int d[4] = {1, 1, 1, 1};
+    return d;
+}
+static inline void tbmd_stub_one_rank(const char *what)
+{
+    if (tbmd_stub_world()[0] > 1) {
+        fprintf(stderr, "mpi stub: %s moves data between ranks; layout mode runs set-up only\n", what);
+        abort();
+    }
+}
+
 static inline int MPI_Init(int *argc, char ***argv) { (void)argc; (void)argv; return MPI_SUCCESS; }
 static inline int MPI_Finalize(void) { return MPI_SUCCESS; }
 static inline int MPI_Initialized(int *flag) { *flag = 1; return MPI_SUCCESS; }
 static inline int MPI_Finalized(int *flag) { *flag = 0; return MPI_SUCCESS; }
-static inline int MPI_Comm_size(MPI_Comm c, int *size) { (void)c; *size = 1; return MPI_SUCCESS; }
-static inline int MPI_Comm_rank(MPI_Comm c, int *rank) { (void)c; *rank = 0; return MPI_SUCCESS; }
+static inline int MPI_Comm_size(MPI_Comm c, int *size) { (void)c; *size = tbmd_stub_world()[0]; return MPI_SUCCESS; }
+static inline int MPI_Comm_rank(MPI_Comm c, int *rank) { (void)c; *rank = tbmd_stub_world()[1]; return MPI_SUCCESS; }
 static inline int MPI_Comm_dup(MPI_Comm c, MPI_Comm *out) { *out = c; return MPI_SUCCESS; }
 static inline int MPI_Comm_free(MPI_Comm *c) { *c = MPI_COMM_NULL; return MPI_SUCCESS; }
 static inline int MPI_Comm_get_parent(MPI_Comm *parent) { *parent = MPI_COMM_NULL; return MPI_SUCCESS; }
@@ -128,6 +164,7 @@ static inline int MPI_Gather(const void *sb, int sc, MPI_Datatype st, void *rb, 
                              MPI_Comm c)
 {
     (void)rc; (void)rt; (void)root; (void)c;
+    tbmd_stub_one_rank("MPI_Gather");
     if (rb && sb && sc > 0) memcpy(rb, sb, (size_t)(sc * tbmd_stub_extent(st)));
     return MPI_SUCCESS;
 }
@@ -135,6 +172,7 @@ static inline int MPI_Gatherv(const void *sb, int sc, MPI_Datatype st, void *rb,
                               MPI_Datatype rt, int root, MPI_Comm c)
 {
     (void)rcs; (void)root; (void)c;
+    tbmd_stub_one_rank("MPI_Gatherv");
     if (rb && sb && sc > 0)
         memcpy((char *)rb + displs[0] * tbmd_stub_extent(rt), sb, (size_t)(sc * tbmd_stub_extent(st)));
     return MPI_SUCCESS;
@@ -142,40 +180,64 @@ static inline int MPI_Gatherv(const void *sb, int sc, MPI_Datatype st, void *rb,
 static inline int MPI_Allreduce(const void *sb, void *rb, int count, MPI_Datatype t, MPI_Op op, MPI_Comm c)
 {
     (void)op; (void)c;
+    tbmd_stub_one_rank("MPI_Allreduce");
     if (sb != rb) memcpy(rb, sb, (size_t)(count * tbmd_stub_extent(t)));
     return MPI_SUCCESS;
 }
 static inline int MPI_Bcast(void *b, int count, MPI_Datatype t, int root, MPI_Comm c)
 {
     (void)b; (void)count; (void)t; (void)root; (void)c;
+    tbmd_stub_one_rank("MPI_Bcast");
     return MPI_SUCCESS;
 }
 
-/* Cartesian topology of one rank: every coordinate is 0 and every shift returns the caller. */
+/* Cartesian topology: periodic, row-major (the last coordinate varies fastest).  With one rank
+ * every coordinate is 0 and every shift returns the caller. */
 static inline int MPI_Cart_create(MPI_Comm old, int nd, const int *dims, const int *periods, int reorder,
                                   MPI_Comm *cart)
 {
-    (void)nd; (void)dims; (void)periods; (void)reorder;
+    (void)periods; (void)reorder;
+    int *g = tbmd_stub_cart();
+    int prod = 1;
+    g[0] = nd;
+    for (int i = 0; i < 3; ++i) g[1 + i] = i < nd ? dims[i] : 1;
+    for (int i = 0; i < nd; ++i) prod *= dims[i];
+    if (nd < 1 || nd > 3 || prod != tbmd_stub_world()[0]) {
+        fprintf(stderr, "mpi stub: Cartesian grid does not match the world size\n");
+        abort();
+    }
     *cart = old;
     return MPI_SUCCESS;
 }
 static inline int MPI_Cart_coords(MPI_Comm c, int rank, int nd, int *coords)
 {
-    (void)c; (void)rank;
-    for (int i = 0; i < nd; ++i) coords[i] = 0;
+    (void)c;
+    const int *g = tbmd_stub_cart();
+    for (int i = nd - 1; i >= 0; --i) {
+        coords[i] = rank % g[1 + i];
+        rank /= g[1 + i];
+    }
     return MPI_SUCCESS;
 }
 static inline int MPI_Cart_rank(MPI_Comm c, const int *coords, int *rank)
 {
-    (void)c; (void)coords;
-    *rank = 0;
+    (void)c;
+    const int *g = tbmd_stub_cart();
+    int r = 0;
+    for (int i = 0; i < g[0]; ++i) r = r * g[1 + i] + ((coords[i] % g[1 + i]) + g[1 + i]) % g[1 + i];
+    *rank = r;
     return MPI_SUCCESS;
 }
 static inline int MPI_Cart_shift(MPI_Comm c, int dir, int disp, int *src, int *dst)
 {
-    (void)c; (void)dir; (void)disp;
-    *src = 0;
-    *dst = 0;
+    const int *g = tbmd_stub_cart();
+    int co[3] = {0, 0, 0};
+    MPI_Cart_coords(c, tbmd_stub_world()[1], g[0], co);
+    const int k = co[dir];
+    co[dir] = k + disp;
+    MPI_Cart_rank(c, co, dst);
+    co[dir] = k - disp;
+    MPI_Cart_rank(c, co, src);
     return MPI_SUCCESS;
 }
 /* A ring shift to oneself: the buffer is sent and received unchanged. */
@@ -183,6 +245,7 @@ static inline int MPI_Sendrecv_replace(void *b, int count, MPI_Datatype t, int d
                                        MPI_Comm c, MPI_Status *st)
 {
     (void)b; (void)count; (void)t; (void)dst; (void)stag; (void)src; (void)rtag; (void)c; (void)st;
+    tbmd_stub_one_rank("MPI_Sendrecv_replace");
     return MPI_SUCCESS;
 }
 

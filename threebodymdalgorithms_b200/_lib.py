@@ -15,7 +15,7 @@ ALGORITHMS = {"nata": NATA, "p3bca": P3BCA, "auta": AUTA}
 PRECISIONS = {"fp64": FP64, "mixed": MIXED}
 
 STATUS = {0: "TBMD_OK", 1: "TBMD_INVALID_ARG", 2: "TBMD_BAD_INPUT", 3: "TBMD_NOT_READY", 4: "TBMD_CAPACITY_RETRY",
-          5: "TBMD_CUDA_ERROR", 6: "TBMD_TIMEOUT", 7: "TBMD_NO_DEVICE", 8: "TBMD_TOO_LARGE"}
+          5: "TBMD_CUDA_ERROR", 6: "TBMD_TIMEOUT", 7: "TBMD_NO_DEVICE", 8: "TBMD_TOO_LARGE", 9: "TBMD_RANK_LAYOUT"}
 NOALLOC_MAX_N = 4096
 
 # every symbol declared in include/tbmd.h
@@ -24,7 +24,7 @@ EXPORTS = ("tbmd_config_init", "tbmd_create", "tbmd_destroy", "tbmd_last_error",
            "tbmd_forces", "tbmd_adjoint", "tbmd_forces_device", "tbmd_adjoint_device", "tbmd_set_domain",
            "tbmd_cells", "tbmd_batch_forces", "tbmd_batch_adjoint", "tbmd_autotune", "tbmd_tuning", "tbmd_sync",
            "tbmd_kernel_launches", "tbmd_set_profiling", "tbmd_phase_times", "tbmd_nata_forces_noalloc",
-           "tbmd_generator_init", "tbmd_generate_particles")
+           "tbmd_generator_init", "tbmd_generate_particles", "tbmd_rank_layout_of")
 PHASES = ("predictor", "cells", "neighbors", "triplets", "update")
 
 
@@ -49,6 +49,13 @@ class Generator(C.Structure):
 
 
 GENERATORS = {"uniform": 0, "clusteredgauss": 1}
+
+
+class RankLayout(C.Structure):
+    """tbmd_rank_layout: the reference's layout of a run on P MPI ranks."""
+    _fields_ = [("world_size", C.c_int32), ("num_dims", C.c_int32), ("dims", C.c_int32 * 3),
+                ("cutoff_boxes", C.c_int32 * 3), ("shift_steps", C.c_int32), ("reserved", C.c_int32),
+                ("cell_size", C.c_double * 3), ("particles_per_rank", C.c_int64), ("dummies", C.c_int64)]
 
 _lib = None
 
@@ -91,6 +98,8 @@ def load():
         "tbmd_nata_forces_noalloc": (C.c_int, [i64, vp, vp, vp, C.c_double, i32, vp, vp, vp, vp]),
         "tbmd_generator_init": (None, [C.POINTER(Generator)]),
         "tbmd_generate_particles": (C.c_int, [vp, C.POINTER(Generator)]),
+        "tbmd_rank_layout_of": (C.c_int, [i32, i32, i32, C.c_double, d, i64, C.POINTER(RankLayout), C.c_char_p,
+                                          i32]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -296,3 +305,24 @@ class Context:
                                        launches.ctypes.data_as(C.POINTER(C.c_uint64)), k)
         return {PHASES[i]: {"ms": float(ms[i]), "calls": int(calls[i]), "launches": int(launches[i])}
                 for i in range(m)}
+
+
+def rank_layout(algorithm: str, world_size: int, n: int, cutoff: float = 0.0, L=None, decomposition: str = "naive"):
+    """Layout of the reference's run of `algorithm` on `world_size` MPI ranks (host only, no GPU):
+    process grid, P3BCA cutoff boxes and shift steps, NATA / AUTA dummy padding, as a dict.  Raises
+    TbmdError(TBMD_RANK_LAYOUT) with the reference's stderr message where that run would stop
+    (tbmd_rank_layout_of, include/tbmd.h)."""
+    if decomposition not in ("naive", "optimal"):
+        raise ValueError("decomposition must be 'naive' or 'optimal'")
+    lib = load()
+    out = RankLayout()
+    msg = C.create_string_buffer(256)
+    Lv = None if L is None else f64(L)
+    st = lib.tbmd_rank_layout_of(ALGORITHMS[algorithm.lower()], int(world_size), int(decomposition == "optimal"),
+                                 float(cutoff), dptr(Lv), int(n), C.byref(out), msg, len(msg))
+    if st != 0:
+        raise TbmdError(st, msg.value.decode() or lib.tbmd_status_string(st).decode())
+    return {"world_size": out.world_size, "num_dims": out.num_dims, "dims": list(out.dims),
+            "cutoff_boxes": list(out.cutoff_boxes), "shift_steps": out.shift_steps,
+            "cell_size": list(out.cell_size), "particles_per_rank": out.particles_per_rank,
+            "dummies": out.dummies}

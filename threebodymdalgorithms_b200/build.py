@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
                   "-I", str(INCLUDE)]
 
-CU_SOURCES = ["tbmd_kernels.cu", "tbmd_api.cu", "tbmd_probe.cu", "tbmd_noalloc.cu", "tbmd_gen.cu"]
+CU_SOURCES = ["tbmd_kernels.cu", "tbmd_api.cu", "tbmd_probe.cu", "tbmd_noalloc.cu", "tbmd_gen.cu", "tbmd_ranks.cpp"]
 
 
 def _stale(target: Path, deps) -> bool:

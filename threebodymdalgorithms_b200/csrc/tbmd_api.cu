@@ -581,6 +581,7 @@ const char *tbmd_status_string(tbmd_status s)
         case TBMD_TIMEOUT: return "device wait timed out";
         case TBMD_NO_DEVICE: return "no sm_100 CUDA device";
         case TBMD_TOO_LARGE: return "n above the allocation-free limit";
+        case TBMD_RANK_LAYOUT: return "the reference's run on that many ranks would stop";
     }
     return "unknown status";
 }

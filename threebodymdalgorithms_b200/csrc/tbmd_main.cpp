@@ -7,7 +7,10 @@
 // value or a value that does not convert prints the help and exits 1, an unknown option is
 // reported and skipped, unset values are 0 and the algorithm defaults to NATA (the reference's
 // zero-initialised globals, main.cpp:27).  Upper-case algorithm names are accepted as well.
-// -decomp and -benchyaml only matter for MPI rank layouts and are accepted and ignored.
+// -benchyaml is accepted and ignored.  -np P lays the run out as the reference would on P MPI
+// ranks (tbmd_rank_layout_of: process grid from -decomp, P3BCA's cutoff-window check, AtomDecomposition
+// padding) and stops where that run stops, with its message and exit status 1; the GPU run itself is
+// the same for every P.  -layoutonly prints that layout as JSON and exits without touching the GPU.
 // GPU options: -prec fp64|mixed, -nu V (AT strength, default 1.0 as main.cpp:41), -device N,
 // -nograph, -tune CACHE.JSONL (autotuner), -dumpfull FILE (state at %.17g after the run),
 // -parseonly (print the parsed arguments as JSON and exit without touching the GPU).
@@ -21,6 +24,7 @@
 // base_<i>.csv with header "ID, pX, pY, pZ, vX, vY, vZ, aX, aY, aZ, m, fX, fY, fZ", rows sorted by
 // ID, values in the default ostream format (6 significant digits).
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -43,6 +47,8 @@ struct Args {
     int algorithm = TBMD_NATA;
     double g[3] = {0.0, 0.0, 0.0};
     bool optimalDecomposition = false;
+    int ranks = 1;            // -np: MPI ranks of the reference run being reproduced
+    bool layoutOnly = false;  // -layoutonly
     // GPU options
     int precision = TBMD_FP64;
     double nu = 1.0;
@@ -67,14 +73,16 @@ void printHelp()
               << "\t-o,--out\t\tcsv base file name that will be used to create all csv outputs from each "
                  "simulation step\n"
               << "-op,--outProfile\t\tjson file to save profile output\n"
-              << "-decomp,--decomp\t\t(optimal | naive) decomposition strategy for cart topology (ignored)\n"
+              << "-decomp,--decomp\t\t(optimal | naive) decomposition strategy for cart topology (with -np)\n"
               << "-benchyaml,--benchyaml\t\tYAML file that contains config for benchmarks (ignored)\n"
               << "\t-c,--cutoff\t\tcutoff distance\n"
               << "GPU options:\n"
               << "\t-prec\t\tfp64 | mixed\n\t-nu\t\tAT strength (1.0)\n\t-device\t\tCUDA device\n"
               << "\t-nograph\t\tno CUDA graph\n\t-tune\t\tautotuner cache file\n"
               << "\t-dumpfull\t\twrite the final state with 17 digits\n\t-opsteps\t\tper-step timings (json lines)\n"
-              << "\t-parseonly\t\tprint parsed args" << std::endl;
+              << "\t-parseonly\t\tprint parsed args\n"
+              << "\t-np\t\tMPI ranks of the reference run to reproduce (layout and checks; default 1)\n"
+              << "\t-layoutonly\t\tprint the rank layout as JSON and exit" << std::endl;
 }
 
 [[noreturn]] void usageExit()
@@ -152,6 +160,11 @@ Args parse(const std::vector<std::string> &args)
                 a.outputSteps = value();
             } else if (isFlag(f, "parseonly", "-parseonly")) {
                 a.parseOnly = true;
+            } else if (isFlag(f, "np", "-np")) {
+                a.ranks = std::stoi(value());
+                if (a.ranks < 1) usageExit();
+            } else if (isFlag(f, "layoutonly", "-layoutonly")) {
+                a.layoutOnly = true;
             } else if (isFlag(f, "h", "-help")) {
                 printHelp();
                 std::exit(0);
@@ -304,10 +317,10 @@ int main(int argc, char **argv)
     if (a.parseOnly) {
         std::printf("{\"algorithm\": \"%s\", \"iterations\": %d, \"delta\": %.17g, \"cutoff\": %.17g, "
                     "\"g\": [%.17g, %.17g, %.17g], \"csv\": \"%s\", \"out\": \"%s\", \"precision\": \"%s\", "
-                    "\"nu\": %.17g, \"device\": %d, \"graph\": %s}\n",
+                    "\"nu\": %.17g, \"device\": %d, \"graph\": %s, \"ranks\": %d, \"decomp\": \"%s\"}\n",
                     algName[a.algorithm], a.iterations, a.deltaT, a.cutoff, a.g[0], a.g[1], a.g[2],
                     a.inputCSV.c_str(), a.outputCSV.c_str(), a.precision == TBMD_MIXED ? "mixed" : "fp64", a.nu,
-                    a.device, a.graph ? "true" : "false");
+                    a.device, a.graph ? "true" : "false", a.ranks, a.optimalDecomposition ? "optimal" : "naive");
         return 0;
     }
     if (!a.benchYaml.empty()) std::cout << "note: -benchyaml is ignored (no MPI benchmark harness)" << std::endl;
@@ -319,6 +332,38 @@ int main(int argc, char **argv)
         return 1;
     }
     const int64_t n = (int64_t)p.id.size();
+
+    if (a.ranks != 1 || a.layoutOnly) {
+        // physical domain size as RegularGridDecomposition::getDomainMinMax takes it
+        // (RegularGridDecomposition.cpp:135-166): the extent widened by 1e-4 on each side
+        double L[3] = {0.0, 0.0, 0.0};
+        for (int d = 0; d < 3 && n > 0; ++d) {
+            const auto mm = std::minmax_element(p.col[d].begin(), p.col[d].end());
+            L[d] = std::fabs((*mm.second + 0.0001) - (*mm.first - 0.0001));
+        }
+        tbmd_rank_layout lay;
+        char msg[256];
+        const tbmd_status ls = tbmd_rank_layout_of(a.algorithm, a.ranks, a.optimalDecomposition ? 1 : 0, a.cutoff,
+                                                   L, n, &lay, msg, (int32_t)sizeof msg);
+        if (ls == TBMD_RANK_LAYOUT) {
+            std::cerr << msg << std::endl;
+            return 1;
+        }
+        if (ls != TBMD_OK) {
+            std::cerr << "error: " << tbmd_status_string(ls) << std::endl;
+            return 1;
+        }
+        if (a.layoutOnly) {
+            std::printf("{\"algorithm\": \"%s\", \"ranks\": %d, \"num_dims\": %d, \"dims\": [%d, %d, %d], "
+                        "\"cutoff_boxes\": [%d, %d, %d], \"shift_steps\": %d, "
+                        "\"cell_size\": [%.17g, %.17g, %.17g], \"particles_per_rank\": %lld, \"dummies\": %lld}\n",
+                        algName[a.algorithm], lay.world_size, lay.num_dims, lay.dims[0], lay.dims[1], lay.dims[2],
+                        lay.cutoff_boxes[0], lay.cutoff_boxes[1], lay.cutoff_boxes[2], lay.shift_steps,
+                        lay.cell_size[0], lay.cell_size[1], lay.cell_size[2], (long long)lay.particles_per_rank,
+                        (long long)lay.dummies);
+            return 0;
+        }
+    }
 
     tbmd_config cfg;
     tbmd_config_init(&cfg);
