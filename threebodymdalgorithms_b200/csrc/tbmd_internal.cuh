@@ -208,14 +208,16 @@ struct SweepWork {
     const int32_t *sys_nblocks;  // [nsys]
 };
 
-// Cell grid of the P3BCA path (one per system).  band/raw_ok parametrise the mixed cutoff test.
+// Cell grid of the P3BCA path (one per system).  band, band64 and raw_ok parametrise the guarded
+// third-edge cutoff test of the triplet kernel.
 struct Grid {
     double L[3], lo[3], w[3];
     int dims[3];
     int64_t ncells;
     double sqcut;
-    float band;   // half-width of the FP32 uncertainty band around cutoff^2
-    int raw_ok;   // every box length >= 4 cutoffs: raw distance = periodic formula for non-wrapping pairs
+    double band64;  // half-width of the FP64 uncertainty band around cutoff^2 (FP64 forms)
+    float band;     // half-width of the FP32 uncertainty band around cutoff^2 (mixed forms)
+    int raw_ok;     // every box length >= 4 cutoffs: raw distance = periodic formula for non-wrapping pairs
 };
 
 // Several independent systems packed back to back: system s owns particles (and sorted slots)

@@ -14,9 +14,9 @@
 //                by cell, stable within a cell.
 //   k_neighbors  half neighbour lists (sorted index t > s) with the reference's exact FP64
 //                periodic cutoff test (structs.hpp:106-115; d == cutoff is inside).
-//   k_p3bca      warp per particle s: all pairs (a < b) of its half list, exact FP64 test of the
-//                third edge, triplet math, per-slot accumulation in shared memory, one FP64 atomic
-//                per list slot.
+//   k_p3bca      warp per particle s: all pairs (a < b) of its half list, guarded cutoff test of the
+//                third edge (exact decision), triplet math, per-slot accumulation in shared memory,
+//                one FP64 atomic per list slot.
 //   k_predictor / k_update   the reference's integrator (structs.hpp:40-99), FP64.
 //
 // Precision: S = double is the FP64 drop-in.  S = float is the mixed form: displacements are
@@ -122,6 +122,12 @@ __device__ __forceinline__ int find_block(const int64_t *prefix, int nblocks, in
     }
     return lo;
 }
+
+// value part as FP64
+__device__ __forceinline__ double to_double(double v) { return v; }
+__device__ __forceinline__ double to_double(float v) { return (double)v; }
+template <class T>
+__device__ __forceinline__ double to_double(Dual<T> v) { return (double)v.v; }
 
 // value part as FP32 (comparisons that only choose between equivalent forms)
 template <class S>
@@ -968,8 +974,7 @@ cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, const
 // (I <= J) queued by the neighbour kernel; long lists are thus spread over many warps and the
 // shared memory of a warp is fixed (two chunks) whatever the list length.  The item's entries are
 // staged as slots in the warp's shared memory: edge from s (hi, its square, and the lo part for the
-// mixed form), an S gradient accumulator per slot, the neighbour index and (FP64 forms) the
-// neighbour's FP64 position for the exact third-edge test.
+// mixed form), an S gradient accumulator per slot and the neighbour index.
 //
 // Every unordered slot pair of the item (all pairs of one chunk, or all pairs across two chunks)
 // is visited once, block by block (blocks of 32 slots).  For own block A
@@ -983,12 +988,12 @@ cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, const
 // broadcast steps the partner gradient is first summed over the warp.  The own-slot gradient stays
 // in registers.  At the end of an item each slot is flushed with one FP64 atomic.
 //
-// Cutoff test of the third edge.  FP64 forms: the reference's exact FP64 test (structs.hpp:106-115)
-// on the staged positions.  Mixed form: the same periodic formula in FP32 on the accurate third
-// edge (or, when no list entry of s wraps around the box and the box is at least 4 cutoffs wide,
-// the raw squared distance, which the formula then equals), decided directly outside a guard band
-// around cutoff^2 that bounds the FP32 error, and by the exact FP64 test inside it.  Counts are
-// therefore exact in both forms.
+// Cutoff test of the third edge: the reference's periodic formula (structs.hpp:106-115) on the third
+// edge the triplet math uses (FP32 in the mixed form, FP64 in the FP64 forms), or, when no list
+// entry of s wraps around the box and the box is at least 4 cutoffs wide, the raw squared distance,
+// which the formula then equals.  Outside a guard band around cutoff^2 that bounds the difference
+// to the reference's own FP64 value the computed distance decides; inside it the reference's exact
+// test on the two neighbours' FP64 positions.  Counts are therefore exact in both forms.
 
 template <class S>
 struct alignas(4 * sizeof(S)) Slot4 {
@@ -1147,12 +1152,10 @@ __device__ __forceinline__ V3<double> slot_gradient<float, double>(const Grad<fl
 template <class S>
 struct SlotLayout {
     // per-warp shared memory, [2 * P3_CHUNK] of each: edge hi + b (Slot4), edge lo (Slot4, mixed only),
-    // FP64 position (3 doubles, FP64 forms only), gradient accumulator (Grad), neighbour index
+    // gradient accumulator (Grad), neighbour index
     static constexpr bool mixed = HasLo<S>::value;
     static constexpr int nlo = mixed ? 1 : 0;
-    static constexpr int npos = mixed ? 0 : 3;
-    static constexpr size_t bytes_per_slot =
-        (1 + nlo) * sizeof(Slot4<S>) + npos * sizeof(double) + sizeof(Grad<S>) + sizeof(int32_t);
+    static constexpr size_t bytes_per_slot = (1 + nlo) * sizeof(Slot4<S>) + sizeof(Grad<S>) + sizeof(int32_t);
 };
 
 
@@ -1160,13 +1163,14 @@ template <class S>
 struct P3Warp {
     Slot4<S> *sd;  // hi edge + b
     Slot4<S> *sl;  // lo edge (mixed)
-    double *px, *py, *pz;
-    Grad<S> *gr;  // gradient accumulators
+    Grad<S> *gr;   // gradient accumulators
     int32_t *idx;
 };
 
-// Third-edge cutoff decision for slots a (own) and b (partner) with third edge w.
-// sq_lo / sq_hi: cutoff^2 minus / plus the FP32 band, hoisted out of the pair loop by the caller.
+// Third-edge cutoff decision for slots a (own) and b (partner) with third edge w (cww = w.w).
+// sq_lo / sq_hi: cutoff^2 minus / plus the FP32 band, hoisted out of the pair loop by the caller
+// (mixed forms).  Outside the band the computed edge decides; inside it the reference's own test
+// on the FP64 positions of the two neighbours.
 template <class S>
 __device__ __forceinline__ bool cut_inside(const P3Warp<S> &W, const CellBufs &cb, const Grid &g, int a, int b,
                                            V3<S> w, S cww, bool rawok, float sq_lo, float sq_hi, float Lx, float Ly,
@@ -1187,7 +1191,19 @@ __device__ __forceinline__ bool cut_inside(const P3Warp<S> &W, const CellBufs &c
         const int32_t ta = W.idx[a], tb = W.idx[b];
         return sqdist_periodic(cb.xs[ta], cb.ys[ta], cb.zs[ta], cb.xs[tb], cb.ys[tb], cb.zs[tb], g) <= g.sqcut;
     }
-    return sqdist_periodic(W.px[a], W.py[a], W.pz[a], W.px[b], W.py[b], W.pz[b], g) <= g.sqcut;
+    // FP64 forms: the same guarded test in FP64 on the FP64 third edge, with the FP64 band
+    double d2;
+    if (rawok) {
+        d2 = to_double(cww);
+    } else {
+        const double ax = fabs(to_double(w.x)), ay = fabs(to_double(w.y)), az = fabs(to_double(w.z));
+        const double mx = fmin(ax, g.L[0] - ax), my = fmin(ay, g.L[1] - ay), mz = fmin(az, g.L[2] - az);
+        d2 = mx * mx + my * my + mz * mz;
+    }
+    if (d2 <= g.sqcut - g.band64) return true;
+    if (d2 > g.sqcut + g.band64) return false;
+    const int32_t ta = W.idx[a], tb = W.idx[b];
+    return sqdist_periodic(cb.xs[ta], cb.ys[ta], cb.zs[ta], cb.xs[tb], cb.ys[tb], cb.zs[tb], g) <= g.sqcut;
 }
 
 // Register cap of the triplet kernel per form.  The mixed forces kernel fits in 64 registers (32
@@ -1233,11 +1249,7 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
     P3Warp<S> W;
     W.sd = (Slot4<S> *)base;
     W.sl = W.sd + SL;
-    double *pbase = (double *)(W.sl + (L::nlo ? SL : 0));
-    W.px = pbase;
-    W.py = pbase + (L::npos ? SL : 0);
-    W.pz = W.py + (L::npos ? SL : 0);
-    W.gr = (Grad<S> *)(W.pz + (L::npos ? SL : 0));
+    W.gr = (Grad<S> *)(W.sl + (L::nlo ? SL : 0));
     W.idx = (int32_t *)(W.gr + SL);
 
     const S nu = constant<S>(nu_d), nu3 = constant<S>(-3.0 * nu_d), nu15 = constant<S>(15.0 * nu_d);
@@ -1282,11 +1294,6 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
             const int32_t t = cb.nbr[(int64_t)s * cap + pos_in_list];
             W.idx[e] = t;
             const double x = cb.xs[t], y = cb.ys[t], z = cb.zs[t];
-            if (L::npos) {
-                W.px[e] = x;
-                W.py[e] = y;
-                W.pz[e] = z;
-            }
             const double ddx = x - xi, ddy = y - yi, ddz = z - zi;
             nowrap = nowrap && fabs(ddx) <= cwrap && fabs(ddy) <= cwrap && fabs(ddz) <= cwrap;
             V3<S> v, l;
@@ -1419,17 +1426,20 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
 
 void fill_grid_test_params(Grid &g);
 
-// Half-width of the FP32 uncertainty band around cutoff^2 of the mixed test.  Each FP32 component
-// of the third edge (two-float difference of edges from i, then L - |d|) is within
-// e = 16 eps32 (max L + cutoff) of the FP64 value; the squared periodic distance is then within
-// 2 sqrt(3) c e + 3 e^2 plus its own FP32 rounding (8 eps32 c^2).  Four times that is used.
-static float guard_band(const Grid &g)
+// Half-width of the uncertainty band around cutoff^2 of the guarded third-edge test, for unit
+// roundoff eps.  Mixed (eps32): each FP32 component of the third edge (two-float difference of edges
+// from i, then L - |d|) is within e = 16 eps (max L + cutoff) of the FP64 value.  FP64 forms
+// (eps64): the third edge is the FP64 difference of two FP64 edges from i, each within eps / 2 of
+// its at most L + cutoff long exact value, so it and the reference's own x_k - x_j (and L - |d|)
+// differ by a few eps (L + cutoff) per component, inside the same e.  The squared periodic
+// distance is then within 2 sqrt(3) c e + 3 e^2 plus its own rounding (8 eps c^2) of the
+// reference's.  Four times that is used.
+static double guard_band(const Grid &g, double eps)
 {
-    const double eps = 1.0 / 8388608.0;  // 2^-23
     const double c = sqrt(g.sqcut);
     const double Lm = fmax(g.L[0], fmax(g.L[1], g.L[2]));
     const double e = 16.0 * eps * (Lm + c);
-    return (float)(4.0 * (2.0 * 1.7320508075688772 * c * e + 3.0 * e * e + 8.0 * eps * g.sqcut));
+    return 4.0 * (2.0 * 1.7320508075688772 * c * e + 3.0 * e * e + 8.0 * eps * g.sqcut);
 }
 
 // The raw squared distance equals the periodic formula for two neighbours of s that do not wrap
@@ -1443,7 +1453,8 @@ static int raw_test_ok(const Grid &g)
 
 void fill_grid_test_params(Grid &g)
 {
-    g.band = guard_band(g);
+    g.band = (float)guard_band(g, 1.0 / 8388608.0);      // 2^-23
+    g.band64 = guard_band(g, 1.0 / 4503599627370496.0);  // 2^-52
     g.raw_ok = raw_test_ok(g);
 }
 
