@@ -320,6 +320,19 @@ def test_clustered_capacity_retry():
     ctx.set_state(st)
     ref, counts = O.simulate("p3bca", 3, st, 0.001, (0.0, -9.81, 0.0), cutoff=2.0, nthreads=0)
     assert counts_close(ctx.step(3), counts, 1e-3)
+    # the same particles again: the grown capacity is kept for this particle count, so the step
+    # runs once, where a fresh context's first step overflows and runs a second time
+    fresh = Context("p3bca", "mixed", 2.0, 0.001, (0, -9.81, 0))
+    fresh.set_state(st)
+    k0 = fresh.kernel_launches()
+    assert fresh.step(1)[0] == counts[0]
+    overflowed = fresh.kernel_launches() - k0
+    fresh.close()
+    for _ in range(2):
+        ctx.set_state(st)
+        k0 = ctx.kernel_launches()
+        assert ctx.step(1)[0] == counts[0]
+        assert ctx.kernel_launches() - k0 < overflowed
     ctx.close()
 
 

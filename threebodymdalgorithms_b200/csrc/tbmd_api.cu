@@ -101,6 +101,11 @@ struct tbmd_ctx {
     int64_t cell_bufs_n = -1, cell_bufs_cells = -1;
     CellBufs cb{};
     int cap = 0;
+    // list capacity of the last complete single-system P3BCA evaluation and its particle count: a
+    // new particle set of the same size starts there instead of at the mean-density estimate, so a
+    // clustered system that is reset and stepped again does not overflow and re-run every time
+    int cap_used = 0;
+    int64_t cap_used_n = -1;
     int p3_warps = 4;
     P3Plan plan{};
     int plan_key[5] = {-1, -1, -1, -1, -1};  // (mixed, dual, energy, cap, warps) the plan was made for
@@ -370,7 +375,10 @@ static tbmd_status ensure_cells(tbmd_ctx *ctx, int64_t n, bool dual, bool energy
     if (!ctx->domain_set)
         return fail(ctx, TBMD_NOT_READY, "P3BCA needs a domain: set particles or call tbmd_set_domain");
     make_grid(ctx);
-    if (ctx->cap == 0) ctx->cap = initial_cap(ctx, n);
+    if (ctx->cap == 0) {
+        ctx->cap = initial_cap(ctx, n);
+        if (ctx->cap_used_n == n && ctx->cap_used > ctx->cap) ctx->cap = ctx->cap_used;
+    }
     // single-system tables: grids[0], cell_off = {0, ncells}, sys_off = {0, n}
     struct {
         Grid g;
@@ -948,6 +956,10 @@ tbmd_status tbmd_step(tbmd_ctx *ctx, int32_t iterations, uint64_t *counts)
                                ctx->stream));
             continue;
         }
+        if (cut) {
+            ctx->cap_used = ctx->cap;
+            ctx->cap_used_n = n;
+        }
         if (counts)
             for (int it = 0; it < iterations; ++it) counts[it] = host[it];
         return TBMD_OK;
@@ -979,7 +991,11 @@ static tbmd_status evaluate(tbmd_ctx *ctx, int64_t n, Pos pos, Out out, bool dua
         CapSeen seen{};
         CK(read_cap_flags(ctx, st, &seen));
         CK(cudaStreamSynchronize(st));
-        if (!grow_caps(ctx, seen)) return TBMD_OK;
+        if (!grow_caps(ctx, seen)) {
+            ctx->cap_used = ctx->cap;
+            ctx->cap_used_n = n;
+            return TBMD_OK;
+        }
     }
     return fail(ctx, TBMD_CAPACITY_RETRY, "neighbour capacity still exceeded after retries (cap %d)", ctx->cap);
 }
