@@ -293,36 +293,48 @@ def run_ours(args, world, rank, local):
         from threebodymdalgorithms_b200._lib import dptr
         lib = ctx._lib
 
-        def e2e_step():
-            ctx._check(lib.tbmd_set_particles(ctx.handle, n, ids.ctypes.data_as(C.POINTER(C.c_int32)),
-                                              *[dptr(pinned[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "ax",
-                                                                          "ay", "az", "m")]))
+        IN = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m")
+        OUT = IN + ("fx", "fy", "fz")
+        ip = C.POINTER(C.c_int32)
+        cnt = np.zeros(1, dtype=np.uint64)
+
+        def e2e_fused():
+            # tbmd_step_host: load, step, read back in one call, the copies overlapping the step
+            ctx._check(lib.tbmd_step_host(ctx.handle, n, ids.ctypes.data_as(ip), *[dptr(pinned[k]) for k in IN], 1,
+                                          cnt.ctypes.data_as(C.POINTER(C.c_uint64)), out_ids.ctypes.data_as(ip),
+                                          *[dptr(outs[k]) for k in OUT]))
+            return int(cnt[0])
+
+        def e2e_separate():
+            ctx._check(lib.tbmd_set_particles(ctx.handle, n, ids.ctypes.data_as(ip), *[dptr(pinned[k]) for k in IN]))
             c = ctx.step(1)
-            ctx._check(lib.tbmd_get_particles(ctx.handle, out_ids.ctypes.data_as(C.POINTER(C.c_int32)),
-                                              *[dptr(outs[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay",
-                                                                        "az", "m", "fx", "fy", "fz")]))
+            ctx._check(lib.tbmd_get_particles(ctx.handle, out_ids.ctypes.data_as(ip), *[dptr(outs[k]) for k in OUT]))
             return int(c[0])
 
-        for _ in range(args.warmup):
-            e2e_step()
-        barrier(world)
-        e2e_ms, e2e_trip = [], 0
-        for _ in range(args.steps):
-            flush.fill_(1.0)
-            torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            e2e_trip += e2e_step()
-            e1.record(stream)
-            e1.synchronize()
-            e2e_ms.append(e0.elapsed_time(e1))
-        barrier(world)
-        tot = allreduce_max(sum(e2e_ms), world)
-        e2e_all = allreduce_sum(float(e2e_trip), world)
+        def e2e_time(fn):
+            for _ in range(args.warmup):
+                fn()
+            barrier(world)
+            ms, trips = [], 0
+            for _ in range(args.steps):
+                flush.fill_(1.0)
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                trips += fn()
+                e1.record(stream)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            barrier(world)
+            return allreduce_max(sum(ms), world), allreduce_sum(float(trips), world)
+
+        tot, e2e_all = e2e_time(e2e_fused)
+        tot_sep, _ = e2e_time(e2e_separate)
         e2e = {"value": e2e_all / (tot * 1e-3), "unit": "triplets/s", "ms_per_step": tot / args.steps,
                "h2d_bytes_per_step": 10 * 8 * n + 4 * n, "d2h_bytes_per_step": 13 * 8 * n + 4 * n,
-               "path": "tbmd_set_particles + tbmd_step(1) + tbmd_get_particles, pinned host buffers"}
+               "path": "tbmd_step_host (state in, step, state out in one C-ABI call), pinned host buffers",
+               "separate_calls_ms_per_step": tot_sep / args.steps}
         ctx.close()
 
     cpu = None

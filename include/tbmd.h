@@ -128,6 +128,23 @@ tbmd_status tbmd_generate_particles(tbmd_ctx *ctx, const tbmd_generator *gen);
  * reference returns from GetNumParticleInteractions(step). */
 tbmd_status tbmd_step(tbmd_ctx *ctx, int32_t iterations, uint64_t *triplets_per_step);
 
+/* tbmd_set_particles, tbmd_step and tbmd_get_particles in one call, for callers whose particles live
+ * in host arrays between steps, as the reference's Simulation keeps them in host vectors
+ * (Simulation.cpp:28-81; its Start loop with a CSV written after every step, Simulation.cpp:74-79).
+ * Inputs as tbmd_set_particles (checked; for P3BCA the domain is taken from them), `iterations`
+ * steps with their triplet counts as tbmd_step, then the state as tbmd_get_particles: any output
+ * may be NULL, and an output may be the very input array of the same field, but outputs must not
+ * overlap one another.  The results are those of the three calls.  What differs is the overlap:
+ * the last step's positions are final once its predictor has run and are copied back while its
+ * forces are computed, masses (which no step changes) and IDs are copied on the host meanwhile,
+ * and the whole call waits on the device once per attempt instead of once per call. */
+tbmd_status tbmd_step_host(tbmd_ctx *ctx, int64_t n, const int32_t *id, const double *x, const double *y,
+                           const double *z, const double *vx, const double *vy, const double *vz, const double *ax,
+                           const double *ay, const double *az, const double *m, int32_t iterations,
+                           uint64_t *triplets_per_step, int32_t *id_out, double *x_out, double *y_out, double *z_out,
+                           double *vx_out, double *vy_out, double *vz_out, double *ax_out, double *ay_out,
+                           double *az_out, double *m_out, double *fx_out, double *fy_out, double *fz_out);
+
 /* Algorithm::SimulationStep alone at the current positions, without integration (how the
  * reference's tests call it, tests.cpp:539).  Writes the stored forces into the context and,
  * if non-NULL, to fx/fy/fz, the total AT energy to *energy, the triplet count to *triplets. */

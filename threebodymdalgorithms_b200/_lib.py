@@ -24,7 +24,7 @@ EXPORTS = ("tbmd_config_init", "tbmd_create", "tbmd_destroy", "tbmd_last_error",
            "tbmd_forces", "tbmd_adjoint", "tbmd_forces_device", "tbmd_adjoint_device", "tbmd_set_domain",
            "tbmd_cells", "tbmd_batch_forces", "tbmd_batch_adjoint", "tbmd_autotune", "tbmd_tuning", "tbmd_sync",
            "tbmd_kernel_launches", "tbmd_set_profiling", "tbmd_phase_times", "tbmd_nata_forces_noalloc",
-           "tbmd_generator_init", "tbmd_generate_particles", "tbmd_rank_layout_of")
+           "tbmd_generator_init", "tbmd_generate_particles", "tbmd_rank_layout_of", "tbmd_step_host")
 PHASES = ("predictor", "cells", "neighbors", "triplets", "update")
 
 
@@ -100,6 +100,7 @@ def load():
         "tbmd_generate_particles": (C.c_int, [vp, C.POINTER(Generator)]),
         "tbmd_rank_layout_of": (C.c_int, [i32, i32, i32, C.c_double, d, i64, C.POINTER(RankLayout), C.c_char_p,
                                           i32]),
+        "tbmd_step_host": (C.c_int, [vp, i64, pi32] + [d] * 10 + [i32, pu64, pi32] + [d] * 13),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -213,6 +214,28 @@ class Context:
         counts = np.zeros(max(iterations, 1), dtype=np.uint64)
         self._check(self._lib.tbmd_step(self._h, int(iterations), counts.ctypes.data_as(C.POINTER(C.c_uint64))))
         return counts[:iterations]
+
+    def step_host(self, st: dict, iterations: int = 1, out: dict | None = None):
+        """Load the particles of `st`, step, and read the state back, in one call (tbmd_step_host):
+        the same results as set_state + step + get_state, with the copies overlapping the step.
+        `out` may give preallocated float64 arrays (any subset of x..fz, and id) to write into.
+        Returns (state dict, per-step triplet counts)."""
+        n = len(st["x"])
+        ins = [f64(st[k]) if st.get(k) is not None else (np.ones(n) if k == "m" else np.zeros(n))
+               for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m")]
+        ids_in = None if st.get("id") is None else np.ascontiguousarray(st["id"], dtype=np.int32)
+        keys = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m", "fx", "fy", "fz")
+        res = dict(out) if out is not None else {k: np.zeros(n) for k in keys}
+        if "id" not in res:
+            res["id"] = np.zeros(n, dtype=np.int32)
+        counts = np.zeros(max(iterations, 1), dtype=np.uint64)
+        ip = C.POINTER(C.c_int32)
+        self._check(self._lib.tbmd_step_host(
+            self._h, n, None if ids_in is None else ids_in.ctypes.data_as(ip), *[dptr(a) for a in ins],
+            int(iterations), counts.ctypes.data_as(C.POINTER(C.c_uint64)), res["id"].ctypes.data_as(ip),
+            *[dptr(res.get(k)) for k in keys]))
+        self.n = n
+        return res, counts[:iterations]
 
     def forces(self):
         n = self.n

@@ -10,6 +10,7 @@
 #include <cstddef>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <new>
 #include <string>
 #include <vector>
@@ -53,6 +54,14 @@ struct tbmd_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // tbmd_step_host: a second stream for the copies that overlap the step, and an event recorded
+    // in every step once the predictor has written the positions (both made on first use)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t pos_event = nullptr;
+    // pinned host words for the per-step counts and the overflow flags read after each step attempt
+    // (a read into pageable memory would block the host until the whole step had finished)
+    void *hstep = nullptr;
+    size_t hstep_bytes = 0;
     std::string err;
     std::string tuning;
     uint64_t launches = 0;
@@ -504,6 +513,7 @@ static tbmd_status enqueue_step(tbmd_ctx *ctx, cudaStream_t st, int *nl)
         CellBufs &cb = ctx->cb;
         phase_mark(ctx, st, PH_CELLS, *nl);  // the predictor runs inside the cell build
         CK(launch_step_cells(n, s, ctx->cfg.dt, ctx->grid, cb, st, nl));
+        if (ctx->pos_event) CK(cudaEventRecordWithFlags(ctx->pos_event, st, cudaEventRecordExternal));
         phase_mark(ctx, st, PH_NEIGHBORS, *nl);
         CK(launch_neighbors(n, ctx->grid, ctx->gset, ctx->ncell_tab.as<int32_t>(), ctx->max_stage, cb, st));
         *nl += 1;
@@ -522,6 +532,7 @@ static tbmd_status enqueue_step(tbmd_ctx *ctx, cudaStream_t st, int *nl)
     phase_mark(ctx, st, PH_PREDICTOR, *nl);
     CK(launch_predictor(n, s[0], s[1], s[2], s[3], s[4], s[5], s[6], ctx->cfg.dt, st));
     *nl += 1;
+    if (ctx->pos_event) CK(cudaEventRecordWithFlags(ctx->pos_event, st, cudaEventRecordExternal));
     // forces of the step's count go to count_cur; the no-cutoff count C(n,3) is added by k_add_u64
     tbmd_status r = enqueue_forces(ctx, n, state_pos(ctx), state_out(ctx), false, nullptr, count_ptr(ctx), st, nl);
     if (r != TBMD_OK) return r;
@@ -652,6 +663,12 @@ void tbmd_destroy(tbmd_ctx *ctx)
                       &ctx->staging, &ctx->long_buf, &ctx->gen_buf, &ctx->bext})
         b->release();
     if (ctx->hpin) cudaFreeHost(ctx->hpin);
+    if (ctx->copy_stream) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+    }
+    if (ctx->hstep) cudaFreeHost(ctx->hstep);
+    if (ctx->pos_event) cudaEventDestroy(ctx->pos_event);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -901,14 +918,19 @@ static bool grow_caps(tbmd_ctx *ctx, const CapSeen &seen)
     return grew;
 }
 
-tbmd_status tbmd_step(tbmd_ctx *ctx, int32_t iterations, uint64_t *counts)
+// Host arrays that receive the state after the steps (tbmd_step_host); NULL entries are skipped.
+struct HostOut {
+    double *dst[13];  // x y z vx vy vz ax ay az m fx fy fz
+};
+
+// The steps of tbmd_step, with the capacity retry.  With `ho`, the state after the last step is
+// also copied to the host: the positions (final once the last step's predictor has run) on the copy
+// stream while the step's forces are computed, velocities, accelerations and forces after the step
+// on the context stream, before the one synchronisation of the attempt.  A retried attempt issues
+// its copies again, so the last (complete) attempt's values are the ones left in the host arrays.
+static tbmd_status run_steps(tbmd_ctx *ctx, int32_t iterations, uint64_t *counts, const HostOut *ho,
+                             const std::function<void()> &while_running = {})
 {
-    if (!ctx) return TBMD_INVALID_ARG;
-    if (iterations < 0) return fail(ctx, TBMD_INVALID_ARG, "iterations < 0");
-    if (ctx->n == 0) return fail(ctx, TBMD_NOT_READY, "no particles set");
-    if (iterations == 0) return TBMD_OK;
-    tbmd_status st = check_device(ctx);
-    if (st != TBMD_OK) return st;
     if (ctx->step_counts_cap < iterations) {
         CK(cudaStreamSynchronize(ctx->stream));
         CK(ctx->step_counts.ensure(sizeof(unsigned long long) * iterations));
@@ -917,6 +939,19 @@ tbmd_status tbmd_step(tbmd_ctx *ctx, int32_t iterations, uint64_t *counts)
     }
     const bool cut = is_p3bca_cut(ctx);
     const int64_t n = ctx->n;
+    const size_t col = sizeof(double) * (size_t)n;
+    const size_t hbytes = sizeof(CapSeen) + 12 + sizeof(unsigned long long) * (size_t)iterations;
+    if (ctx->hstep_bytes < hbytes) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (ctx->hstep) CK(cudaFreeHost(ctx->hstep));
+        ctx->hstep = nullptr;
+        ctx->hstep_bytes = 0;
+        CK(cudaHostAlloc(&ctx->hstep, hbytes, cudaHostAllocDefault));
+        ctx->hstep_bytes = hbytes;
+    }
+    CapSeen *hseen = (CapSeen *)ctx->hstep;
+    unsigned long long *hcounts = (unsigned long long *)((char *)ctx->hstep + 32);  // 8-byte aligned
+    tbmd_status st = TBMD_OK;
     for (int attempt = 0; attempt < 4; ++attempt) {
         void *before[5] = {ctx->state.p, ctx->nbr_buf.p, ctx->cell_n.p, ctx->prefix.p, ctx->long_buf.p};
         st = prepare(ctx, n, false, false);
@@ -944,12 +979,23 @@ tbmd_status tbmd_step(tbmd_ctx *ctx, int32_t iterations, uint64_t *counts)
                 ctx->launches += nl;
             }
         }
-        std::vector<unsigned long long> host(iterations);
-        CapSeen seen{};
-        CK(cudaMemcpyAsync(host.data(), ctx->step_counts.p, sizeof(unsigned long long) * iterations,
+        if (ho) {
+            // the last recorded position event belongs to the last step just enqueued
+            CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->pos_event, 0));
+            for (int k = 0; k < 3; ++k)
+                if (ho->dst[k])
+                    CK(cudaMemcpyAsync(ho->dst[k], ctx->s[k], col, cudaMemcpyDeviceToHost, ctx->copy_stream));
+            for (int k = 3; k < 13; ++k)
+                if (k != 9 && ho->dst[k])
+                    CK(cudaMemcpyAsync(ho->dst[k], ctx->s[k], col, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        CK(cudaMemcpyAsync(hcounts, ctx->step_counts.p, sizeof(unsigned long long) * iterations,
                            cudaMemcpyDeviceToHost, ctx->stream));
-        CK(read_cap_flags(ctx, ctx->stream, &seen));
+        CK(read_cap_flags(ctx, ctx->stream, hseen));
+        if (attempt == 0 && while_running) while_running();  // host work that overlaps the device
         CK(cudaStreamSynchronize(ctx->stream));
+        if (ho) CK(cudaStreamSynchronize(ctx->copy_stream));
+        const CapSeen seen = *hseen;
         phase_resolve(ctx);
         if (cut && grow_caps(ctx, seen)) {
             CK(cudaMemcpyAsync(ctx->s[0], ctx->snapshot.p, sizeof(double) * 9 * n, cudaMemcpyDeviceToDevice,
@@ -961,10 +1007,58 @@ tbmd_status tbmd_step(tbmd_ctx *ctx, int32_t iterations, uint64_t *counts)
             ctx->cap_used_n = n;
         }
         if (counts)
-            for (int it = 0; it < iterations; ++it) counts[it] = host[it];
+            for (int it = 0; it < iterations; ++it) counts[it] = hcounts[it];
         return TBMD_OK;
     }
     return fail(ctx, TBMD_CAPACITY_RETRY, "neighbour capacity still exceeded after retries (cap %d)", ctx->cap);
+}
+
+tbmd_status tbmd_step(tbmd_ctx *ctx, int32_t iterations, uint64_t *counts)
+{
+    if (!ctx) return TBMD_INVALID_ARG;
+    if (iterations < 0) return fail(ctx, TBMD_INVALID_ARG, "iterations < 0");
+    if (ctx->n == 0) return fail(ctx, TBMD_NOT_READY, "no particles set");
+    if (iterations == 0) return TBMD_OK;
+    tbmd_status st = check_device(ctx);
+    if (st != TBMD_OK) return st;
+    return run_steps(ctx, iterations, counts, nullptr);
+}
+
+tbmd_status tbmd_step_host(tbmd_ctx *ctx, int64_t n, const int32_t *id, const double *x, const double *y,
+                           const double *z, const double *vx, const double *vy, const double *vz, const double *ax,
+                           const double *ay, const double *az, const double *m, int32_t iterations,
+                           uint64_t *triplets_per_step, int32_t *id_out, double *x_out, double *y_out, double *z_out,
+                           double *vx_out, double *vy_out, double *vz_out, double *ax_out, double *ay_out,
+                           double *az_out, double *m_out, double *fx_out, double *fy_out, double *fz_out)
+{
+    if (!ctx) return TBMD_INVALID_ARG;
+    if (iterations < 0) return fail(ctx, TBMD_INVALID_ARG, "iterations < 0");
+    tbmd_status st = check_device(ctx);
+    if (st != TBMD_OK) return st;
+    if (!ctx->copy_stream) {
+        CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ctx->pos_event, cudaEventDisableTiming));
+        invalidate_graph(ctx);  // the step graph gains the position event
+    }
+    st = tbmd_set_particles(ctx, n, id, x, y, z, vx, vy, vz, ax, ay, az, m);
+    if (st != TBMD_OK) return st;
+    HostOut ho{{x_out, y_out, z_out, vx_out, vy_out, vz_out, ax_out, ay_out, az_out, m_out, fx_out, fy_out, fz_out}};
+    // masses (no step changes them) and IDs come from the inputs, on the host, while the GPU works
+    auto host_columns = [&]() {
+        if (m_out && m_out != m) std::memmove(m_out, m, sizeof(double) * (size_t)n);
+        if (id_out && id_out != ctx->id.data()) std::memcpy(id_out, ctx->id.data(), sizeof(int32_t) * (size_t)n);
+    };
+    if (iterations == 0) {
+        for (int k = 0; k < 13; ++k)
+            if (k != 9 && ho.dst[k])
+                CK(cudaMemcpyAsync(ho.dst[k], ctx->s[k], sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+        host_columns();
+        CK(cudaStreamSynchronize(ctx->stream));
+        return TBMD_OK;
+    }
+    // the host copies run while the first attempt's device work is in flight
+    return run_steps(ctx, iterations, triplets_per_step, &ho, host_columns);
 }
 
 // Forward (dual = false) or adjoint (dual = true) evaluation with capacity retry, on ctx's state
