@@ -819,7 +819,9 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(const __grid_const
         }
         __syncthreads();
         const int T = cpre[32];
-        const bool staged = T <= max_stage;
+        // staged: the candidates and, after them, 32 far-away sentinels, so that a warp's scan
+        // needs no bounds test (a lane past T reads a sentinel, which fails the cutoff)
+        const bool staged = T + 32 <= max_stage;
         // candidate q lies in table entry k: the largest k with cpre[k] <= q (empty entries have
         // cpre[k] == cpre[k + 1] and are skipped by taking the largest)
         auto entry_of = [&](int q) {
@@ -830,12 +832,18 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(const __grid_const
             return k;
         };
         if (staged) {
-            for (int q = threadIdx.x; q < T; q += NB_THREADS) {
-                const int k = entry_of(q);
-                const int t = cstart[k] + (q - cpre[k]);
-                shi[q] = qhi[t];
-                slo[q] = qlo[t];
-                st[q] = t;
+            for (int q = threadIdx.x; q < T + 32; q += NB_THREADS) {
+                if (q < T) {
+                    const int k = entry_of(q);
+                    const int t = cstart[k] + (q - cpre[k]);
+                    shi[q] = qhi[t];
+                    slo[q] = qlo[t];
+                    st[q] = t;
+                } else {
+                    shi[q] = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+                    slo[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    st[q] = -1;
+                }
             }
         }
         __syncthreads();
@@ -845,42 +853,71 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(const __grid_const
             const float4 oh = staged ? shi[sl] : qhi[s], ol = staged ? slo[sl] : qlo[s];
             int cnt = 0;
             int32_t *dst = nbr + (int64_t)s * cap;
-            for (int q0 = sl + 1; q0 < T; q0 += 32) {
-                const int q = q0 + lane;
-                bool pass = false;
-                int t = 0;
-                if (q < T) {
-                    float4 h;
-                    if (staged) {
-                        t = st[q];
-                        h = shi[q];
-                    } else {
-                        const int k = entry_of(q);
-                        t = cstart[k] + (q - cpre[k]);
-                        h = qhi[t];
-                    }
-                    float d2;
-                    if (raw) {
-                        // every coordinate lies in the box: the hi parts alone are within 2^-24 L, and
-                        // the periodic form is the raw distance (each axis under 2 cells <= L / 2)
-                        const float dx = h.x - oh.x, dy = h.y - oh.y, dz = h.z - oh.z;
-                        d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                    } else {
-                        const float4 l = staged ? slo[q] : qlo[t];
-                        const float dx = (h.x - oh.x) + (l.x - ol.x), dy = (h.y - oh.y) + (l.y - ol.y),
-                                    dz = (h.z - oh.z) + (l.z - ol.z);
-                        const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
-                        const float mx = fminf(ax, Lx - ax), my = fminf(ay, Ly - ay), mz = fminf(az, Lz - az);
-                        d2 = fmaf(mx, mx, fmaf(my, my, mz * mz));
-                    }
-                    pass = d2 <= sq_lo;
-                    if (!pass && d2 <= sq_hi)
-                        pass = sqdist_periodic(xs[s], ys[s], zs[s], xs[t], ys[t], zs[t], G) <= G.sqcut;
-                }
+            // one candidate per lane and iteration; the pass mask compacts the list in order
+            auto emit = [&](bool pass, int t) {
                 const unsigned m = __ballot_sync(0xffffffffu, pass);
                 const int off = cnt + __popc(m & ((1u << lane) - 1u));
                 if (pass && off < cap) dst[off] = t;
                 cnt += __popc(m);
+            };
+            auto exact = [&](int t) {
+                return sqdist_periodic(xs[s], ys[s], zs[s], xs[t], ys[t], zs[t], G) <= G.sqcut;
+            };
+            if (staged && raw) {
+                // every coordinate lies in the box: the hi parts alone are within 2^-24 L, and the
+                // periodic form is the raw distance (each axis under 2 cells <= L / 2)
+                for (int q0 = sl + 1; q0 < T; q0 += 32) {
+                    const int q = q0 + lane;
+                    const float4 h = shi[q];
+                    const int t = st[q];
+                    const float dx = h.x - oh.x, dy = h.y - oh.y, dz = h.z - oh.z;
+                    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    bool pass = d2 <= sq_lo;
+                    if (!pass && d2 <= sq_hi) pass = exact(t);
+                    emit(pass, t);
+                }
+            } else if (staged) {
+                for (int q0 = sl + 1; q0 < T; q0 += 32) {
+                    const int q = q0 + lane;
+                    const float4 h = shi[q], l = slo[q];
+                    const int t = st[q];
+                    const float dx = (h.x - oh.x) + (l.x - ol.x), dy = (h.y - oh.y) + (l.y - ol.y),
+                                dz = (h.z - oh.z) + (l.z - ol.z);
+                    const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
+                    const float mx = fminf(ax, Lx - ax), my = fminf(ay, Ly - ay), mz = fminf(az, Lz - az);
+                    const float d2 = fmaf(mx, mx, fmaf(my, my, mz * mz));
+                    bool pass = d2 <= sq_lo;
+                    if (!pass && d2 <= sq_hi) pass = exact(t);
+                    emit(pass, t);
+                }
+            } else {
+                // more candidates than the staging holds: read them from global memory
+                for (int q0 = sl + 1; q0 < T; q0 += 32) {
+                    const int q = q0 + lane;
+                    bool pass = false;
+                    int t = 0;
+                    if (q < T) {
+                        const int k = entry_of(q);
+                        t = cstart[k] + (q - cpre[k]);
+                        const float4 h = qhi[t];
+                        float d2;
+                        if (raw) {
+                            const float dx = h.x - oh.x, dy = h.y - oh.y, dz = h.z - oh.z;
+                            d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        } else {
+                            const float4 l = qlo[t];
+                            const float dx = (h.x - oh.x) + (l.x - ol.x), dy = (h.y - oh.y) + (l.y - ol.y),
+                                        dz = (h.z - oh.z) + (l.z - ol.z);
+                            const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
+                            const float mx = fminf(ax, Lx - ax), my = fminf(ay, Ly - ay),
+                                        mz = fminf(az, Lz - az);
+                            d2 = fmaf(mx, mx, fmaf(my, my, mz * mz));
+                        }
+                        pass = d2 <= sq_lo;
+                        if (!pass && d2 <= sq_hi) pass = exact(t);
+                    }
+                    emit(pass, t);
+                }
             }
             if (lane == 0) nbr_count[s] = cnt;
             warp_max = cnt > warp_max ? cnt : warp_max;
