@@ -48,8 +48,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         _run(cmd)
     main_deps = [CSRC / "tbmd_main.cpp", INCLUDE / "tbmd.h", LIB]
     if (CSRC / "tbmd_main.cpp").exists() and (force or _stale(MAIN, main_deps)):
-        cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-I", str(INCLUDE), str(CSRC / "tbmd_main.cpp"), "-o", str(MAIN),
-               "-L", str(PKG), "-ltbmd", "-Wl,-rpath,$ORIGIN"]
+        cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-pthread", "-I", str(INCLUDE), str(CSRC / "tbmd_main.cpp"), "-o",
+               str(MAIN), "-L", str(PKG), "-ltbmd", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd))
         _run(cmd)

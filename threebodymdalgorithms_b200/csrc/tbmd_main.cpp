@@ -33,6 +33,7 @@
 #include <numeric>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "tbmd.h"
@@ -245,19 +246,42 @@ bool fetch(tbmd_ctx *ctx, int64_t n, State &s)
                               s.v[9].data(), s.v[10].data(), s.v[11].data(), s.v[12].data()) == TBMD_OK;
 }
 
-// utility.cpp:54-68 (writeStepToCSVWithForces), rows sorted by ID (Simulation.cpp:127-128).
-void writeStepCSV(const std::string &path, const State &s)
+// Rows in ID order (Simulation.cpp:127-128).  IDs do not change between steps, so the order is
+// computed once.
+std::vector<size_t> idOrder(const std::vector<int32_t> &id)
 {
-    std::vector<size_t> order(s.id.size());
+    std::vector<size_t> order(id.size());
     std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return s.id[a] < s.id[b]; });
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return id[a] < id[b]; });
+    return order;
+}
+
+// utility.cpp:54-68 (writeStepToCSVWithForces): the reference's header and columns, each value as
+// std::ostream prints it by default.  The rows are formatted by several threads, each into its own
+// stream with the same default formatting, and written in order.
+void writeStepCSV(const std::string &path, const State &s, const std::vector<size_t> &order)
+{
+    const size_t n = order.size();
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t nt = std::max<size_t>(1, std::min<size_t>({hw ? hw : 1u, 16u, (n + 4095) / 4096}));
+    std::vector<std::string> parts(nt);
+    auto format = [&](size_t t) {
+        std::ostringstream o;
+        for (size_t r = n * t / nt; r < n * (t + 1) / nt; ++r) {
+            const size_t i = order[r];
+            o << s.id[i];
+            for (int k = 0; k < 13; ++k) o << ", " << s.v[k][i];
+            o << "\n";
+        }
+        parts[t] = o.str();
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < nt; ++t) pool.emplace_back(format, t);
+    format(0);
+    for (auto &th : pool) th.join();
     std::ofstream out(path);
     out << "ID, pX, pY, pZ, vX, vY, vZ, aX, aY, aZ, m, fX, fY, fZ\n";
-    for (size_t i : order) {
-        out << s.id[i];
-        for (int k = 0; k < 13; ++k) out << ", " << s.v[k][i];
-        out << "\n";
-    }
+    for (const std::string &part : parts) out << part;
 }
 
 void writeFull(const std::string &path, const State &s, const std::vector<uint64_t> &counts)
@@ -400,6 +424,9 @@ int main(int argc, char **argv)
     std::vector<long long> stepNs;
     std::vector<std::vector<long long>> phaseNs;  // [step][phase], device time of each GPU phase
     State s;
+    State states[2];          // per-step CSV output: two host buffers, one being written out
+    std::thread writer[2];
+    std::vector<size_t> order;
     const bool profile = !a.outputProfile.empty();
     if (n > 0 && a.iterations > 0) {
         const bool perStep = !a.outputCSV.empty() || profile || !a.outputSteps.empty();
@@ -421,10 +448,17 @@ int main(int argc, char **argv)
                     phaseNs.push_back(row);
                 }
                 if (!a.outputCSV.empty()) {
-                    if (!fetch(ctx, n, s)) die("get_particles");
-                    writeStepCSV(stepPath(a.outputCSV, i), s);
+                    // the previous step's file is written in the background while this step ran;
+                    // its buffer is fetched into again only after that write has finished
+                    State &buf = states[i % 2];
+                    if (writer[i % 2].joinable()) writer[i % 2].join();
+                    if (!fetch(ctx, n, buf)) die("get_particles");
+                    if (order.empty()) order = idOrder(buf.id);
+                    writer[i % 2] = std::thread(writeStepCSV, stepPath(a.outputCSV, i), std::cref(buf), std::cref(order));
                 }
             }
+            for (auto &w : writer)
+                if (w.joinable()) w.join();
             if (profile) tbmd_set_profiling(ctx, 0);
         } else {
             counts.resize(a.iterations);
