@@ -186,6 +186,32 @@ def barrier(world):
         torch.cuda.synchronize()
 
 
+# Algorithmic bytes per particle of the P3BCA step's cell build (predictor fused in), each array
+# access counted once: k_predict_assign reads x, y, z, vx, vy, vz, ax (56 B), writes x, y, z (24 B)
+# and the cell index (4 B), and adds to the cell's count (8 B); k_scatter_gather reads the cell
+# index, its start and fill counter (16 B) and x, y, z (24 B), and writes the sorted index (4 B),
+# the sorted FP64 positions (24 B) and their FP32 hi/lo copies (32 B).  The scan over the cells
+# adds under 1 B per particle.
+CELL_BUILD_BYTES = 92 + 100
+
+
+def hbm_peak():
+    """(GB/s, source): the measured copy bandwidth in MEASURED_PEAKS.json, else the pool's fallback."""
+    try:
+        return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback"
+
+
+def cell_build_roofline(phase, n):
+    ms = phase["ms"] / max(phase["calls"], 1)
+    peak, src = hbm_peak()
+    gbs = CELL_BUILD_BYTES * n / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+    return {"bound": "hbm", "kernels": "k_predict_assign, k_cell_scan, k_scatter_gather", "ms": round(ms, 5),
+            "bytes_per_particle": CELL_BUILD_BYTES, "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(gbs / peak, 4), "peak_source": src}
+
+
 def timed_steps(ctx, steps, flush, torch, reset=None):
     """Per-step CUDA-event times (ms) on the context's stream.  Before each step (untimed) the
     workload's input state is restored, so every step is the same step of the same input, and L2
@@ -279,6 +305,8 @@ def run_ours(args, world, rank, local):
                 "kernel_ms": round(kern_ms, 5), "flop_per_triplet": FLOP_PER_TRIPLET,
                 "peak_source": "measured on this GPU by tbmd_probe_fma_tflops (FMA = 2 FLOP)",
                 "phases_ms_per_step": {k: round(v["ms"] / max(v["calls"], 1), 5) for k, v in main["phases"].items()}}
+    if w["algorithm"] == "p3bca" and w["cutoff"] > 0:
+        roofline["cell_build"] = cell_build_roofline(main["phases"]["cells"], n)
 
     # end to end through the C ABI with host buffers (pinned), per step: state in, step, state out
     e2e = None
