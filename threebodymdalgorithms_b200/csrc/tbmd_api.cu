@@ -86,6 +86,7 @@ struct tbmd_ctx {
     DevBuf sweep_sys;  // single system: sys_items[2], sys_off[2], sys_prefix[1], sys_nblocks[1]
     DevBuf prefix;
     int prefix_JB = 0, prefix_alg = -1;
+    int64_t prefix_kseg = 0;  // k range per AUTA item of the current work list (0: the whole sweep)
     int64_t prefix_n = -1;
     int nblocks = 0;
     int64_t total_items = 0;
@@ -231,13 +232,29 @@ static void phase_resolve(tbmd_ctx *ctx)
     ctx->cur_phase = -1;
 }
 
-// Work list of the no-cutoff sweep for (algorithm, n, R).
+// Work list of the no-cutoff sweep for (algorithm, n, R).  A small AUTA system has fewer (block, i)
+// items than the GPU has resident warps, and their k sweeps differ in length by the whole system, so
+// the longest one sets the kernel time: its items are then split by k range (kseg particles each),
+// the longest range that still gives every resident warp four items.
 static tbmd_status ensure_sweep(tbmd_ctx *ctx, int alg, int64_t n, int R, bool dual)
 {
     const int JB = 32 * R;
-    if (ctx->prefix_n != n || ctx->prefix_JB != JB || ctx->prefix_alg != alg) {
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    int per_sm = 2048 / sweep_block_size(alg, mixed(ctx), dual, R);  // resident blocks bounded below by registers
+    if (per_sm < 1) per_sm = 1;
+    ctx->sweep_grid = sms * per_sm;
+    int64_t kseg = 0;
+    if (alg == TBMD_AUTA) {
+        const int64_t want = 4ll * ctx->sweep_grid * (sweep_block_size(alg, mixed(ctx), dual, R) / 32);
+        if (sweep_items(alg, n, JB, nullptr) < want) {
+            for (kseg = 256; kseg > 32 && sweep_items(alg, n, JB, nullptr, kseg) < want; kseg /= 2) {
+            }
+        }
+    }
+    if (ctx->prefix_n != n || ctx->prefix_JB != JB || ctx->prefix_alg != alg || ctx->prefix_kseg != kseg) {
         std::vector<int64_t> pre((size_t)(n / JB + 3), 0);
-        int64_t total = sweep_items(alg, n, JB, pre.data());
+        int64_t total = sweep_items(alg, n, JB, pre.data(), kseg);
         int64_t nb = n >= 3 ? (n - 2 + JB) / JB : 0;
         if (total >= (int64_t)UINT32_MAX - 65536)
             return fail(ctx, TBMD_INVALID_ARG, "n = %lld gives too many sweep work items", (long long)n);
@@ -247,6 +264,7 @@ static tbmd_status ensure_sweep(tbmd_ctx *ctx, int alg, int64_t n, int R, bool d
         ctx->prefix_n = n;
         ctx->prefix_JB = JB;
         ctx->prefix_alg = alg;
+        ctx->prefix_kseg = kseg;
         ctx->nblocks = (int)nb;
         ctx->total_items = total;
         // one system: sys_items = {0, total}, sys_off = {0, n}, sys_prefix = {0}, sys_nblocks = {nb}
@@ -259,12 +277,6 @@ static tbmd_status ensure_sweep(tbmd_ctx *ctx, int alg, int64_t n, int R, bool d
         CK(cudaStreamSynchronize(ctx->stream));
         if (alg == TBMD_NATA) CK(ctx->partial.ensure(sizeof(double) * 3 * (size_t)n * (size_t)(nb > 0 ? nb : 1)));
     }
-    int per_sm = 0, sms = 0;
-    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    (void)dual;
-    per_sm = 2048 / sweep_block_size(alg, mixed(ctx), dual, R);  // resident blocks bounded below by registers
-    if (per_sm < 1) per_sm = 1;
-    ctx->sweep_grid = sms * per_sm;
     return TBMD_OK;
 }
 
@@ -274,7 +286,7 @@ static SweepWork single_sweep(tbmd_ctx *ctx)
     const char *t = ctx->sweep_sys.as<char>();
     return SweepWork{ctx->prefix.as<int64_t>(), ctx->nblocks, ctx->total_items, sweep_counter(ctx), 1,
                      (const int64_t *)t, (const int64_t *)(t + 16), (const int64_t *)(t + 32),
-                     (const int32_t *)(t + 40)};
+                     (const int32_t *)(t + 40), ctx->prefix_kseg};
 }
 
 // Cell grid for the current domain and cutoff (oracle tbo_cell_dims).

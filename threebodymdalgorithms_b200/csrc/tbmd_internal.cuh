@@ -206,6 +206,7 @@ struct SweepWork {
     const int64_t *sys_off;      // [nsys + 1] first particle of each system
     const int64_t *sys_prefix;   // [nsys] start of each system's block prefix in `prefix`
     const int32_t *sys_nblocks;  // [nsys]
+    int64_t kseg;                // AUTA: k range of one item (a multiple of 32), 0 = to the system's end
 };
 
 // Cell grid of the P3BCA path (one per system).  band, band64 and raw_ok parametrise the guarded
@@ -235,7 +236,7 @@ void fill_grid_test_params(Grid &g);
 // Launchers (tbmd_kernels.cu).  All take the stream they run on and return the launch error.
 
 int sweep_block_size(int algorithm, bool mixed, bool dual, int R);
-int64_t sweep_items(int algorithm, int64_t n, int JB, int64_t *prefix_host /* nb+1 or NULL */);
+int64_t sweep_items(int algorithm, int64_t n, int JB, int64_t *prefix_host /* nb+1 or NULL */, int64_t kseg = 0);
 // energy_out: one accumulator per system (index = system)
 
 cudaError_t launch_auta(bool mixed, bool dual, int R, bool energy, int64_t n, Pos pos, Out out, double *energy_out,

@@ -167,7 +167,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
         const int64_t off = work.sys_off[sys], hi = work.sys_off[sys + 1];
         const int64_t *prefix = work.prefix + work.sys_prefix[sys];
         const int b = find_block(prefix, work.sys_nblocks[sys], wl);
-        const int64_t i = off + wl - prefix[b];
+        // item -> (i, k range): the whole sweep from the block, or one segment of it
+        int64_t i = off + wl - prefix[b], kbeg = off + (int64_t)b * JB, kend = hi;
+        if (work.kseg > 0) {
+            const int64_t r = wl - prefix[b], nseg = (hi - kbeg + work.kseg - 1) / work.kseg;
+            i = off + r / nseg;
+            kbeg += (r % nseg) * work.kseg;
+            kend = min(hi, kbeg + work.kseg);
+        }
         const double xi = pos.x[i], yi = pos.y[i], zi = pos.z[i];
         double dxi = 0.0, dyi = 0.0, dzi = 0.0;
         if (Traits<S>::dual) {
@@ -192,9 +199,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
         }
         V3<Acc> fi = widen(vzero<S>());
         Acc en_item = to_acc(szero<S>());
-        for (int64_t kt = off + (int64_t)b * JB; kt < hi; kt += 32) {
+        for (int64_t kt = kbeg; kt < kend; kt += 32) {
             const int64_t k = kt + lane;
-            const bool kv = k < hi;
+            const bool kv = k < kend;
             V3<S> vk = vzero<S>(), vkl = vzero<S>();
             if (kv) edge<S>(pos, k, xi, yi, zi, dxi, dyi, dzi, vk, vkl);
             {
@@ -226,7 +233,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
                 const int64_t kidx = kt + kk;
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    const bool valid = jv[r] && kidx > jj[r] && kidx < hi;
+                    const bool valid = jv[r] && kidx > jj[r] && kidx < kend;
                     V3<S> ec;  // third edge x_k - x_j
                     const ATCoef<S> cf = triplet<ENERGY>(u[r], ul[r], aa[r], v, vl, e.b, nu, nu3, nu15, valid, en, ec);
                     al[r] = al[r] + cf.alpha;
@@ -393,16 +400,18 @@ __global__ void k_nata_reduce(int64_t n, int nb, const double *__restrict__ part
 
 constexpr int SWEEP_WARPS = 8;
 
-int64_t sweep_items(int algorithm, int64_t n, int JB, int64_t *prefix)
+int64_t sweep_items(int algorithm, int64_t n, int JB, int64_t *prefix, int64_t kseg)
 {
     // AUTA (algorithm 2): block b = [b*JB, (b+1)*JB) needs j <= n-2 and i < j, so it has
-    // min((b+1)*JB - 1, n - 2) items i = 0 ..; NATA (0): every block with j <= n-2 pairs with all n i.
+    // min((b+1)*JB - 1, n - 2) values i = 0 ..; NATA (0): every block with j <= n-2 pairs with all n i.
+    // With kseg > 0 (AUTA) each (block, i) is split into ceil((n - b*JB) / kseg) items by k range.
     int64_t nb = n >= 3 ? (n - 2 + JB) / JB : 0;  // blocks holding some j <= n - 2
     int64_t total = 0;
     if (prefix) prefix[0] = 0;
     for (int64_t b = 0; b < nb; ++b) {
         int64_t cnt = algorithm == 0 ? n : std::min<int64_t>((b + 1) * JB - 1, n - 2);
         if (cnt < 0) cnt = 0;
+        if (algorithm != 0 && kseg > 0) cnt *= (n - b * JB + kseg - 1) / kseg;
         total += cnt;
         if (prefix) prefix[b + 1] = total;
     }
