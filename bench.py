@@ -312,11 +312,17 @@ def run_ours(args, world, rank, local):
     e2e = None
     if not args.no_e2e:
         ctx = new_ctx(args.precision)
-        pinned = {k: torch.from_numpy(np.ascontiguousarray(st[k], dtype=np.float64)).pin_memory().numpy()
-                  for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m")}
+        # one pinned SoA block per direction, a row per field (the library copies back-to-back fields
+        # in one transfer)
+        in_keys = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m")
+        out_keys = in_keys + ("fx", "fy", "fz")
+        in_block = torch.empty((len(in_keys), n), dtype=torch.float64).pin_memory().numpy()
+        out_block = torch.empty((len(out_keys), n), dtype=torch.float64).pin_memory().numpy()
+        pinned = {k: in_block[r] for r, k in enumerate(in_keys)}
+        for k in in_keys:
+            pinned[k][:] = st[k]
         ids = torch.from_numpy(np.asarray(st["id"], dtype=np.int32)).pin_memory().numpy()
-        outs = {k: torch.empty(n, dtype=torch.float64).pin_memory().numpy()
-                for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m", "fx", "fy", "fz")}
+        outs = {k: out_block[r] for r, k in enumerate(out_keys)}
         out_ids = torch.empty(n, dtype=torch.int32).pin_memory().numpy()
         from threebodymdalgorithms_b200._lib import dptr
         lib = ctx._lib
@@ -361,7 +367,7 @@ def run_ours(args, world, rank, local):
         tot_sep, _ = e2e_time(e2e_separate)
         e2e = {"value": e2e_all / (tot * 1e-3), "unit": "triplets/s", "ms_per_step": tot / args.steps,
                "h2d_bytes_per_step": 10 * 8 * n + 4 * n, "d2h_bytes_per_step": 13 * 8 * n + 4 * n,
-               "path": "tbmd_step_host (state in, step, state out in one C-ABI call), pinned host buffers",
+               "path": "tbmd_step_host (state in, step, state out in one C-ABI call), pinned host SoA blocks",
                "separate_calls_ms_per_step": tot_sep / args.steps}
         ctx.close()
 
