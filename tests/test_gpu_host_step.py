@@ -100,3 +100,30 @@ def test_step_host_after_a_capacity_retry():
     got, c = ctx.step_host(st, 2)
     check_same(ref, cref, got, c, 2, "fp64")
     ctx.close()
+
+
+def test_contiguous_field_blocks():
+    """Fields given as the rows of one block (x, y, z, vx, ... back to back in memory) move in one
+    transfer per contiguous run; the results are those of separate arrays, through tbmd_step_host
+    and through tbmd_set_particles / tbmd_get_particles alike."""
+    st = uniform_input("p3bca")
+    n = len(st["x"])
+    ins = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m")
+    block_in = np.empty((len(ins), n))
+    for r, k in enumerate(ins):
+        block_in[r] = st[k] if k in st else (np.ones(n) if k == "m" else np.zeros(n))
+    rows_in = {k: block_in[r] for r, k in enumerate(ins)}
+    rows_in["id"] = st["id"]
+    ref, cref = separate("p3bca", "fp64", 2.0, st, 1)
+    block_out = np.zeros((len(KEYS), n))
+    out = {k: block_out[r] for r, k in enumerate(KEYS)}
+    ctx = Context("p3bca", "fp64", 2.0, 0.001, G)
+    got, c = ctx.step_host(rows_in, 1, out=out)
+    check_same(ref, cref, got, c, 1, "fp64")
+    # the same block through the separate calls
+    ctx.set_state(rows_in)
+    assert ctx.step(1)[0] == cref[0]
+    back = ctx.get_state()
+    for k in KEYS:
+        assert rel(back[k], ref[k]) <= 1e-12, k
+    ctx.close()
