@@ -45,6 +45,8 @@ WORKLOADS = {
                   algorithm="p3bca", n=131072, cutoff=1.5, gen="uniform"),
     "c2": dict(desc="AUTA, N=8192 uniform in 20^3, no cutoff", algorithm="auta", n=8192, cutoff=0.0, gen="uniform",
                box=20.0),
+    "c2nata": dict(desc="NATA, N=8192 uniform in 20^3, no cutoff", algorithm="nata", n=8192, cutoff=0.0,
+                   gen="uniform", box=20.0),
     "c1": dict(desc="AUTA, N=512 uniform in 10^3, no cutoff", algorithm="auta", n=512, cutoff=0.0, gen="uniform",
                box=10.0),
     "c4": dict(desc="P3BCA, N=262144 clustered Gaussian (256 clusters, sigma 1) in 64^3, cutoff 2",
@@ -52,7 +54,7 @@ WORKLOADS = {
     "c5": dict(desc="64 systems, N uniform in 512..4096 at density 2.048, batched AUTA and P3BCA (cutoff 2), "
                     "forward and adjoint", algorithm="batch", n=0, cutoff=2.0, gen="batch"),
 }
-FLOP_PER_TRIPLET = 120  # the fixed, formulation-independent per-triplet credit (BASELINE convention)
+FLOP_PER_TRIPLET = 120  # the fixed, formulation-independent credit per triplet inside the cutoff
 DT, G = 0.001, (0.0, -9.81, 0.0)
 
 

@@ -1,7 +1,7 @@
 /*
  * CPU oracle for the Axilrod-Teller three-body hot path of dmartin13/ThreeBodyMDAlgorithms.
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker the CUDA path is compared against; it is
+ * TEST INFRASTRUCTURE ONLY.  This file is the oracle the CUDA path is compared against; it is
  * never linked into the product library, and nothing in the product calls it.  Only tests/, the
  * smoke check and bench.py's CPU-baseline leg load it (through oracle/oracle.py).
  *
