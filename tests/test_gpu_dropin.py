@@ -55,3 +55,21 @@ def test_cli_mixed_and_dump(tmp_path):
     assert forces["time unit"] == "nanosecond" and len(forces["times per proc"]["0"]) == 2
     assert all(t > 0 for t in forces["times per proc"]["0"])
     assert prof["hitrate"]["avg hitrate per sim step"][0] == pytest.approx(12982 / math.comb(512, 3))
+
+
+def test_cli_np_gives_the_same_results(tmp_path):
+    """-np P reproduces the reference's P-rank set-up but computes the same triplets on the GPU: the
+    NATA run (a deterministic sweep) writes the same bytes for P = 1 and P = 3, and so does a P3BCA
+    run whose cutoff window is valid at P = 3 (the counts are exact; the files agree to 6 digits)."""
+    inp = GOLDEN / "p3bca_n512_c2_3steps.csv"
+    for P in ("1", "3"):
+        d = tmp_path / f"np{P}"
+        d.mkdir()
+        run_main(["-a", "nata", "-i", "2", "-d", "0.001", "-gy", "-9.81", "-np", P, "-csv", str(inp),
+                  "-o", str(d / "o.csv")], d)
+        run_main(["-a", "p3bca", "-i", "2", "-c", "1.0", "-d", "0.001", "-gy", "-9.81", "-np", P,
+                  "-dumpfull", str(d / "p3.txt"), "-csv", str(inp)], d)
+    assert (tmp_path / "np1" / "o_1.csv").read_bytes() == (tmp_path / "np3" / "o_1.csv").read_bytes()
+    counts = [[l for l in (tmp_path / f"np{P}" / "p3.txt").read_text().splitlines() if l.startswith("step")]
+              for P in ("1", "3")]
+    assert counts[0] == counts[1] and len(counts[0]) == 2
