@@ -93,3 +93,42 @@ def test_cli_errors_like_reference():
 def test_cli_missing_input_fails():
     r = subprocess.run([str(MAIN), "-csv", "/nonexistent.csv", "-i", "1"], capture_output=True, text=True)
     assert r.returncode == 1
+
+
+def _summary(path):
+    r = subprocess.run([str(MAIN), "-csv", str(path), "-inputsummary"], capture_output=True, text=True)
+    return r.returncode, r.stdout, r.stderr
+
+
+@pytest.mark.parametrize("name", ["c1_auta_n512.csv", "p3bca_n512_c2_3steps.csv"])
+def test_dropin_reads_csv_like_the_reference(name, tmp_path):
+    """The drop-in's parallel CSV reader gives exactly what a correctly rounded parse gives (the
+    reference reads with strtod semantics), also with blank lines, CRLF line ends and extra columns."""
+    src = GOLDEN / name
+    lines = src.read_text().splitlines()
+    messy = tmp_path / "messy.csv"
+    body = [lines[0]] + [l + ", 7, 8" if i % 3 == 0 else l for i, l in enumerate(lines[1:])]
+    body.insert(5, "   ")
+    body.insert(9, "")
+    messy.write_bytes(("\r\n".join(body) + "\r\n").encode())
+    ref = csvio.read_particles(str(src))
+    for path in (src, messy):
+        rc, out, err = _summary(path)
+        assert rc == 0, err
+        d = json.loads(out)
+        assert d["n"] == len(ref["x"]) and d["id_sum"] == int(np.sum(ref["id"]))
+        for k, key in enumerate(("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m")):
+            col = ref[key]
+            assert d["columns"][k] == [col[0], col[-1], col.min(), col.max()], key
+
+
+def test_dropin_csv_errors(tmp_path):
+    head = "ID, pX, pY, pZ, vX, vY, vZ, aX, aY, aZ, m\n"
+    good = "0, 1, 2, 3, 0, 0, 0, 0, 0, 0, 1\n"
+    for body, msg in ((good + "1, 2, 3\n", "row 1 has fewer than 11 columns"),
+                      (good + good + "x, 1, 2, 3, 0, 0, 0, 0, 0, 0, 1\n", "row 2: bad ID"),
+                      (good + "1, 1, oops, 3, 0, 0, 0, 0, 0, 0, 1\n", "row 1: bad number ' oops'")):
+        f = tmp_path / "bad.csv"
+        f.write_text(head + body)
+        rc, out, err = _summary(f)
+        assert rc == 1 and msg in err, (rc, err)

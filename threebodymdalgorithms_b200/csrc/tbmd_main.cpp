@@ -26,7 +26,9 @@
 #include <algorithm>
 #include <cmath>
 #include <chrono>
+#include <cstdint>
 #include <cstdio>
+#include <cstring>
 #include <cstdlib>
 #include <fstream>
 #include <iostream>
@@ -50,6 +52,7 @@ struct Args {
     bool optimalDecomposition = false;
     int ranks = 1;            // -np: MPI ranks of the reference run being reproduced
     bool layoutOnly = false;  // -layoutonly
+    bool inputSummary = false;  // -inputsummary
     // GPU options
     int precision = TBMD_FP64;
     double nu = 1.0;
@@ -83,7 +86,8 @@ void printHelp()
               << "\t-dumpfull\t\twrite the final state with 17 digits\n\t-opsteps\t\tper-step timings (json lines)\n"
               << "\t-parseonly\t\tprint parsed args\n"
               << "\t-np\t\tMPI ranks of the reference run to reproduce (layout and checks; default 1)\n"
-              << "\t-layoutonly\t\tprint the rank layout as JSON and exit" << std::endl;
+              << "\t-layoutonly\t\tprint the rank layout as JSON and exit\n"
+              << "\t-inputsummary\t\tprint what was read from -csv as JSON and exit" << std::endl;
 }
 
 [[noreturn]] void usageExit()
@@ -166,6 +170,8 @@ Args parse(const std::vector<std::string> &args)
                 if (a.ranks < 1) usageExit();
             } else if (isFlag(f, "layoutonly", "-layoutonly")) {
                 a.layoutOnly = true;
+            } else if (isFlag(f, "inputsummary", "-inputsummary")) {
+                a.inputSummary = true;
             } else if (isFlag(f, "h", "-help")) {
                 printHelp();
                 std::exit(0);
@@ -184,46 +190,92 @@ struct Particles {
     std::vector<double> col[10];  // x y z vx vy vz ax ay az m
 };
 
-// utility.cpp:14-24: header row, then ID and 10 numeric columns; further columns are ignored.
+// utility.cpp:14-24: header row, then ID and 10 numeric columns; further columns are ignored.  Blank
+// lines are skipped (and not counted as rows), a trailing carriage return is dropped, each cell is
+// read with strtol / strtod from its start (leading blanks allowed), and the first bad row is
+// reported.  The file is read at once and its rows are parsed by several threads.
 bool readCSV(const std::string &path, Particles &p, std::string &err)
 {
-    std::ifstream in(path);
-    if (!in) {
+    FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) {
         err = "cannot open " + path;
         return false;
     }
-    std::string line;
-    std::getline(in, line);  // header
-    size_t row = 0;
-    while (std::getline(in, line)) {
-        if (!line.empty() && line.back() == '\r') line.pop_back();
-        if (line.find_first_not_of(" \t") == std::string::npos) continue;
-        std::vector<std::string> cells;
-        std::stringstream ss(line);
-        std::string c;
-        while (std::getline(ss, c, ',')) cells.push_back(c);
-        if (cells.size() < 11) {
-            err = "row " + std::to_string(row) + " has fewer than 11 columns";
-            return false;
-        }
-        char *end = nullptr;
-        long idv = std::strtol(cells[0].c_str(), &end, 10);
-        if (end == cells[0].c_str()) {
-            err = "row " + std::to_string(row) + ": bad ID";
-            return false;
-        }
-        p.id.push_back((int32_t)idv);
-        for (int k = 0; k < 10; ++k) {
-            const char *b = cells[k + 1].c_str();
-            double v = std::strtod(b, &end);
-            if (end == b) {
-                err = "row " + std::to_string(row) + ": bad number '" + cells[k + 1] + "'";
-                return false;
-            }
-            p.col[k].push_back(v);
-        }
-        ++row;
+    std::string buf;
+    std::fseek(f, 0, SEEK_END);
+    const long size = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    if (size > 0) {
+        buf.resize((size_t)size);
+        const size_t got = std::fread(&buf[0], 1, (size_t)size, f);
+        buf.resize(got);
     }
+    std::fclose(f);
+    // the rows: every non-blank line after the header, as [begin, end) without the line break
+    std::vector<std::pair<size_t, size_t>> rows;
+    size_t pos = buf.find('\n');
+    pos = pos == std::string::npos ? buf.size() : pos + 1;  // skip the header line
+    while (pos < buf.size()) {
+        size_t e = buf.find('\n', pos);
+        if (e == std::string::npos) e = buf.size();
+        size_t le = e;
+        if (le > pos && buf[le - 1] == '\r') --le;
+        if (buf.find_first_not_of(" \t", pos) < le) rows.emplace_back(pos, le);
+        pos = e + 1;
+    }
+    const size_t n = rows.size();
+    p.id.assign(n, 0);
+    for (auto &c : p.col) c.assign(n, 0.0);
+    struct Bad {
+        size_t row = SIZE_MAX;
+        std::string msg;
+    };
+    auto parse = [&](size_t r0, size_t r1, Bad &bad) {
+        for (size_t r = r0; r < r1; ++r) {
+            const char *b = buf.data() + rows[r].first, *e = buf.data() + rows[r].second;
+            const char *cell[11];
+            int nc = 0;
+            for (const char *q = b; nc < 11;) {
+                cell[nc++] = q;
+                q = (const char *)std::memchr(q, ',', (size_t)(e - q));
+                if (!q) break;
+                ++q;
+            }
+            if (nc < 11) {
+                bad = {r, "row " + std::to_string(r) + " has fewer than 11 columns"};
+                return;
+            }
+            char *end = nullptr;
+            const long idv = std::strtol(cell[0], &end, 10);
+            if (end == cell[0]) {
+                bad = {r, "row " + std::to_string(r) + ": bad ID"};
+                return;
+            }
+            p.id[r] = (int32_t)idv;
+            for (int k = 0; k < 10; ++k) {
+                const double v = std::strtod(cell[k + 1], &end);
+                if (end == cell[k + 1]) {
+                    const char *ce = (const char *)std::memchr(cell[k + 1], ',', (size_t)(e - cell[k + 1]));
+                    bad = {r, "row " + std::to_string(r) + ": bad number '" +
+                                  std::string(cell[k + 1], ce ? ce : e) + "'"};
+                    return;
+                }
+                p.col[k][r] = v;
+            }
+        }
+    };
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t nt = std::max<size_t>(1, std::min<size_t>({hw ? hw : 1u, 16u, (n + 8191) / 8192}));
+    std::vector<Bad> bads(nt);
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < nt; ++t) pool.emplace_back(parse, n * t / nt, n * (t + 1) / nt, std::ref(bads[t]));
+    parse(0, n / nt, bads[0]);
+    for (auto &th : pool) th.join();
+    for (const Bad &bd : bads)
+        if (bd.row != SIZE_MAX) {  // chunks are in row order: the first one found is the first bad row
+            err = bd.msg;
+            return false;
+        }
     return true;
 }
 
@@ -356,6 +408,21 @@ int main(int argc, char **argv)
         return 1;
     }
     const int64_t n = (int64_t)p.id.size();
+    if (a.inputSummary) {
+        // what was read, for checks without a GPU: the row count, and per column the first, last,
+        // smallest and largest value (%.17g), plus the ID sum
+        long long idsum = 0;
+        for (int32_t v : p.id) idsum += v;
+        std::printf("{\"n\": %lld, \"id_sum\": %lld, \"columns\": [", (long long)n, idsum);
+        for (int k = 0; k < 10; ++k) {
+            const auto &c = p.col[k];
+            const auto mm = n ? std::minmax_element(c.begin(), c.end()) : std::make_pair(c.begin(), c.begin());
+            std::printf("%s[%.17g, %.17g, %.17g, %.17g]", k ? ", " : "", n ? c.front() : 0.0, n ? c.back() : 0.0,
+                        n ? *mm.first : 0.0, n ? *mm.second : 0.0);
+        }
+        std::printf("]}\n");
+        return 0;
+    }
 
     if (a.ranks != 1 || a.layoutOnly) {
         // physical domain size as RegularGridDecomposition::getDomainMinMax takes it
