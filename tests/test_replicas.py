@@ -43,7 +43,7 @@ def _rank_main(rank, world, port, out):
 def test_replica_aggregation_two_gloo_ranks():
     world = 2
     port = _free_port()
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:  # no fork of this multi-threaded process
         out = mgr.dict()
         mp.spawn(_rank_main, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)
