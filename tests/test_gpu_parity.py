@@ -223,6 +223,74 @@ def test_p3bca_particles_outside_the_domain():
         ctx.close()
 
 
+def cutoff_triangles(c, L, seed):
+    """Isolated triangles: apex s, base j-k of length c (1 + r)^(1/2) in a random direction of the
+    x-y plane, so that the base's squared length sits r (relatively) inside or outside cutoff^2,
+    with r cycling through 1e-12 .. 1e-5 and a random sign.  The random direction makes the FP32
+    rounding of the edges generic (an axis-aligned base of a short binary length would round to
+    exactly cutoff^2).  The apex lies one cell layer below its base, so it comes first in the cell
+    order and the triplet kernel's third-edge test decides the base; the list test sees only the
+    two sides of 0.9.  In every other row the last triangle straddles the periodic boundary in x,
+    and the first row's bases cross it in y (the wrapped form of the test).  Triangles are at
+    least 2.25 apart (> c) from one another, also across the periodic boundaries of the L^3 box
+    with cells of c = L / 20."""
+    rng = np.random.default_rng(seed)
+    rel = np.array([1e-12, 1e-9, 1e-7, 1e-6, 3e-6, 1e-5])
+    nx, ny, nz = 7, 8, 10
+    pts, r_of = [], []
+    for iz in range(nz):
+        for iy in range(ny):
+            straddle = iy % 2 == 0
+            for ix in range(nx):
+                if straddle and ix == 0:
+                    continue
+                r = rel[len(r_of) % len(rel)] * rng.choice([-1.0, 1.0])
+                half = c * math.sqrt(1.0 + r) / 2
+                last = straddle and ix == nx - 1
+                th = rng.uniform(-1.0, 1.0) if last else rng.uniform(0.0, 2 * math.pi)  # cos >= 0.54
+                hx, hy = half * math.cos(th), half * math.sin(th)
+                px = L - 0.3 if last else ix * L / nx + 1.0
+                py, pz = iy * L / ny + 0.5, iz * 3.0 + 1.4
+                pts += [(px, py, pz), ((px - hx) % L, (py - hy) % L, pz + 0.5),
+                        ((px + hx) % L, (py + hy) % L, pz + 0.5)]
+                r_of.append(r)
+    return np.array(pts), np.array(r_of)
+
+
+def test_p3bca_third_edges_at_the_cutoff():
+    """Forces, counts and the adjoint (FP64 and mixed) include exactly the triangles the
+    reference's FP64 test includes, d^2 <= cutoff^2 on the FP64 positions, with bases as close as
+    1e-12 to the cutoff: far inside the FP32 uncertainty of the mixed forms' third edge, whose
+    guard band then defers to the exact test.  A triangle left out has exactly zero forces and
+    adjoint.  The mixed adjoint is within 1e-5 of the FP64 one."""
+    c, L = 1.5, 30.0
+    P, r = cutoff_triangles(c, L, 17)
+    st = {"x": P[:, 0].copy(), "y": P[:, 1].copy(), "z": P[:, 2].copy()}
+    box, lo = np.full(3, L), np.zeros(3)
+    fx, fy, fz, c_ref = O.forces(st["x"], st["y"], st["z"], 1.0, c, box, lo, nthreads=0)
+    ref = np.stack([fx, fy, fz], 1)
+    inside = r < 0
+    assert c_ref == inside.sum()  # every base on its intended side of the cutoff
+    per_triangle = lambda a: np.abs(a.reshape(-1, 3, 3)).sum((1, 2)) > 0
+    assert np.array_equal(per_triangle(ref), inside)
+    gf = np.random.default_rng(3).normal(size=P.shape)
+    adj = {}
+    for prec, tol in (("fp64", FP64_TOL), ("mixed", MIXED_FORCE_TOL)):
+        ctx = Context("p3bca", prec, c)
+        ctx.set_state(st)
+        ctx.set_domain(box, lo)
+        gfx, gfy, gfz, e, cnt = ctx.forces()
+        f = np.stack([gfx, gfy, gfz], 1)
+        assert cnt == c_ref, (prec, cnt, c_ref)
+        assert np.array_equal(per_triangle(f), inside), prec
+        assert rel_l2(f, ref) <= tol, prec
+        gx, gy, gz, _ = ctx.adjoint(gf[:, 0], gf[:, 1], gf[:, 2], 0.0)
+        adj[prec] = np.stack([gx, gy, gz], 1)
+        assert np.array_equal(per_triangle(adj[prec]), inside), prec
+        ctx.close()
+    assert rel_l2(adj["mixed"], adj["fp64"]) <= MIXED_FORCE_TOL
+
+
 @pytest.mark.parametrize("algo", ["p3bca", "auta", "nata"])
 def test_mixed_forces_near_coincident_pairs(algo):
     """Pairs 1e-3 apart, planted beside random particles, carry the largest forces of the system.

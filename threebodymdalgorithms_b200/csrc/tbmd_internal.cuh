@@ -209,15 +209,17 @@ struct SweepWork {
     int64_t kseg;                // AUTA: k range of one item (a multiple of 32), 0 = to the system's end
 };
 
-// Cell grid of the P3BCA path (one per system).  band, band64 and raw_ok parametrise the guarded
-// third-edge cutoff test of the triplet kernel.
+// Cell grid of the P3BCA path (one per system).  band, band64, raw_lo / raw_hi and raw_ok
+// parametrise the guarded cutoff tests of the list and triplet kernels.
 struct Grid {
     double L[3], lo[3], w[3];
     int dims[3];
     int64_t ncells;
     double sqcut;
     double band64;  // half-width of the FP64 uncertainty band around cutoff^2 (FP64 forms)
-    float band;     // half-width of the FP32 uncertainty band around cutoff^2 (mixed forms)
+    float band;     // half-width of the FP32 uncertainty band around cutoff^2 (FP32 geometry)
+    float raw_lo;   // FP32 third-edge test without wrapping, hi + lo edges: d2 <= raw_lo is inside,
+    float raw_hi;   // d2 > raw_hi outside, the exact test in between
     int raw_ok;     // every box length >= 4 cutoffs: raw distance = periodic formula for non-wrapping pairs
 };
 

@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 #include "tbmd_internal.cuh"
 
@@ -1214,16 +1215,17 @@ struct P3Warp {
 };
 
 // Third-edge cutoff decision for slots a (own) and b (partner) with third edge w (cww = w.w).
-// sq_lo / sq_hi: cutoff^2 minus / plus the FP32 band, hoisted out of the pair loop by the caller
-// (mixed forms).  Outside the band the computed edge decides; inside it the reference's own test
-// on the FP64 positions of the two neighbours.
+// sq_lo / sq_hi: the FP32 thresholds (cutoff^2 minus / plus the band of the item's test form),
+// hoisted out of the pair loop by the caller (FP32 geometry: the mixed forces and the mixed
+// adjoint).  Outside the band the computed edge decides; inside it the reference's own test on the
+// FP64 positions of the two neighbours.
 template <class S>
 __device__ __forceinline__ bool cut_inside(const P3Warp<S> &W, const CellBufs &cb, const Grid &g, int a, int b,
                                            V3<S> w, S cww, bool rawok, float sq_lo, float sq_hi, float Lx, float Ly,
                                            float Lz)
 {
     // g is the system's grid (L and cutoff of the exact test)
-    if (SlotLayout<S>::mixed) {
+    if (std::is_same<typename Traits<S>::T, float>::value) {
         float d2;
         if (rawok) {
             d2 = to_float(cww);
@@ -1330,7 +1332,6 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
         }
         const Grid &G = set.nsys > 1 ? set.grids[sys] : g;
         const float Lx = (float)G.L[0], Ly = (float)G.L[1], Lz = (float)G.L[2];
-        const float sq_lo = (float)G.sqcut - G.band, sq_hi = (float)G.sqcut + G.band;
         const int Ms = mI + mJ;
         const double xi = cb.xs[s], yi = cb.ys[s], zi = cb.zs[s];
         const double dxi = dual ? cb.dxs[s] : 0.0, dyi = dual ? cb.dys[s] : 0.0, dzi = dual ? cb.dzs[s] : 0.0;
@@ -1351,6 +1352,11 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
             W.gr[e] = grad_zero<S>();
         }
         const bool rawok = G.raw_ok && __all_sync(0xffffffffu, nowrap);
+        // FP32 thresholds: the narrow band of hi + lo edges that do not wrap (mixed forces), else
+        // the band of FP32 geometry with wrapping or without lo parts (the mixed adjoint)
+        const bool narrow = rawok && L::mixed;
+        const float sq_lo = narrow ? G.raw_lo : (float)G.sqcut - G.band;
+        const float sq_hi = narrow ? G.raw_hi : (float)G.sqcut + G.band;
         __syncwarp();
         S en = szero<S>();
 
@@ -1497,10 +1503,26 @@ static int raw_test_ok(const Grid &g)
     return (g.L[0] >= 4.0 * c && g.L[1] >= 4.0 * c && g.L[2] >= 4.0 * c) ? 1 : 0;
 }
 
+// Half-width of the band of the FP32 third-edge test of an item whose neighbours do not wrap, with
+// hi + lo edges (mixed forces).  Each edge from s is formed in FP64 (components within the cutoff
+// c) and split into hi + lo floats, exact to 2^-48 c.  A third-edge component
+// w = (v_hi - u_hi) + (v_lo - u_lo) is then within 2^-23 |w| + 2^-45 c of the difference of the FP64
+// edges: the hi difference rounds to within 2^-24 of itself and lies within 2^-23 c of w (the lo
+// parts), the lo difference to within 2^-47 c, and the sum rounds once.  The squared length (one
+// product and two FMAs over positive terms, three roundings) is then within
+// (2^-22 + 3 * 2^-24) |w|^2 + 2^-42 c^2 of the squared FP64 difference, which is within 2^-46 c^2 of
+// the reference's sum of squares of x_k - x_j (raw here: |w| <= 2 c <= L / 2).  Near cutoff^2 all of
+// that is below 8 * 2^-24 c^2, and the thresholds themselves round to within 2^-24 c^2 in FP32.
+// Four times the sum, 36 * 2^-24 c^2, is used.  It is independent of the box length, unlike the
+// band of the wrapped form, whose L - |d| carries errors of order 2^-24 L.
+static double raw_band(const Grid &g) { return 36.0 / 16777216.0 * g.sqcut; }  // 2^-24
+
 void fill_grid_test_params(Grid &g)
 {
     g.band = (float)guard_band(g, 1.0 / 8388608.0);      // 2^-23
     g.band64 = guard_band(g, 1.0 / 4503599627370496.0);  // 2^-52
+    g.raw_lo = (float)(g.sqcut - raw_band(g));
+    g.raw_hi = (float)(g.sqcut + raw_band(g));
     g.raw_ok = raw_test_ok(g);
 }
 
