@@ -257,20 +257,47 @@ def cutoff_triangles(c, L, seed):
     return np.array(pts), np.array(r_of)
 
 
-def test_p3bca_third_edges_at_the_cutoff():
+def cutoff_sides(c, L, seed):
+    """Isolated triangles whose side s-j from the apex is c (1 + r)^(1/2) long (r as in
+    cutoff_triangles), in a random direction rising 0.2 c to 0.93 c in z, with k 0.9 from both:
+    the apex is alone in the first cell layer of its triangle, so the list kernel's pair test
+    decides s-j and the triplet is counted exactly when s-j is inside.  A lattice of 8^3 triangles
+    4.5 apart in the L = 36 box (cells of c = 1.5); its first column's sides cross the periodic
+    boundary in x when they point to -x."""
+    rng = np.random.default_rng(seed)
+    rel = np.array([1e-12, 1e-9, 1e-7, 1e-6, 3e-6, 1e-5])
+    pts, r_of = [], []
+    for iz in range(8):
+        for iy in range(8):
+            for ix in range(8):
+                r = rel[len(r_of) % len(rel)] * rng.choice([-1.0, 1.0])
+                cp = c * math.sqrt(1.0 + r)
+                th, cz = rng.uniform(0.0, 2 * math.pi), rng.uniform(0.2, 0.93)
+                sz = math.sqrt(1.0 - cz * cz)
+                d = np.array([sz * math.cos(th), sz * math.sin(th), cz])
+                nrm = np.array([-math.sin(th), math.cos(th), 0.0])
+                s0 = np.array([ix * 4.5 + 1.0, iy * 4.5 + 1.0, iz * 4.5 + 1.4])
+                pts += [s0, (s0 + cp * d) % L, (s0 + 0.5 * cp * d + 0.5 * nrm) % L]
+                r_of.append(r)
+    return np.array(pts), np.array(r_of)
+
+
+@pytest.mark.parametrize("family,L", [("third edge", 30.0), ("side", 36.0)])
+def test_p3bca_edges_at_the_cutoff(family, L):
     """Forces, counts and the adjoint (FP64 and mixed) include exactly the triangles the
-    reference's FP64 test includes, d^2 <= cutoff^2 on the FP64 positions, with bases as close as
-    1e-12 to the cutoff: far inside the FP32 uncertainty of the mixed forms' third edge, whose
-    guard band then defers to the exact test.  A triangle left out has exactly zero forces and
+    reference's FP64 test includes, d^2 <= cutoff^2 on the FP64 positions, with one edge as close
+    as 1e-12 to the cutoff: far inside the FP32 uncertainty of the mixed forms, whose guard bands
+    then defer to the exact test.  The near edge is the third edge (the triplet kernel's test) or
+    a side from the apex (the list kernel's).  A triangle left out has exactly zero forces and
     adjoint.  The mixed adjoint is within 1e-5 of the FP64 one."""
-    c, L = 1.5, 30.0
-    P, r = cutoff_triangles(c, L, 17)
+    c = 1.5
+    P, r = cutoff_triangles(c, L, 17) if family == "third edge" else cutoff_sides(c, L, 19)
     st = {"x": P[:, 0].copy(), "y": P[:, 1].copy(), "z": P[:, 2].copy()}
     box, lo = np.full(3, L), np.zeros(3)
     fx, fy, fz, c_ref = O.forces(st["x"], st["y"], st["z"], 1.0, c, box, lo, nthreads=0)
     ref = np.stack([fx, fy, fz], 1)
     inside = r < 0
-    assert c_ref == inside.sum()  # every base on its intended side of the cutoff
+    assert c_ref == inside.sum()  # every near edge on its intended side of the cutoff
     per_triangle = lambda a: np.abs(a.reshape(-1, 3, 3)).sum((1, 2)) > 0
     assert np.array_equal(per_triangle(ref), inside)
     gf = np.random.default_rng(3).normal(size=P.shape)
