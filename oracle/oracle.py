@@ -15,6 +15,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "liboracle.so"
 REF_DIR = HERE / "_ref"
+# where the reference's sources are read when present (the build container only)
+REFERENCE_ROOT = Path("/root/reference")
+STUB_INCLUDE = HERE / "refstub" / "inc"  # stand-in mpi.h and Eigen/Dense for the reference's headers
 
 ALGORITHMS = {"nata": 0, "p3bca": 1, "auta": 2}
 
@@ -30,7 +33,7 @@ def build(force: bool = False) -> Path:
     return LIB_PATH
 
 
-def build_reference(ref_root: str = "/root/reference", jobs: int = 8) -> bool:
+def build_reference(ref_root: str = str(REFERENCE_ROOT), jobs: int = 8) -> bool:
     """Build oracle/_ref from the reference sources with oracle/Makefile.ref; False if absent."""
     if not Path(ref_root, "src").is_dir():
         return (REF_DIR / "ref_dump").exists()
