@@ -841,6 +841,8 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(const __grid_const
                 if (k + step < 27 && cpre[k + step] <= q) k += step;
             return k;
         };
+        // read before the barrier below: warp 0 rewrites raw_cell for its next cell once past it
+        const bool raw = raw_cell != 0;
         if (staged) {
             for (int q = threadIdx.x; q < T + 32; q += NB_THREADS) {
                 if (q < T) {
@@ -857,7 +859,6 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(const __grid_const
             }
         }
         __syncthreads();
-        const bool raw = raw_cell != 0;
         for (int sl = warp; sl < e0 - b0; sl += NW) {
             const int s = b0 + sl;  // cell c comes first in the candidate order: q = sl
             const float4 oh = staged ? shi[sl] : qhi[s], ol = staged ? slo[sl] : qlo[s];
