@@ -1360,79 +1360,114 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
         const float sq_hi = narrow ? G.raw_hi : (float)G.sqcut + G.band;
         __syncwarp();
         S en = szero<S>();
-
-        for (int A0 = 0; A0 < mI; A0 += 32) {
-            const int mA = min(32, mI - A0);
-            const bool own = lane < mA;
-            const int a = A0 + (own ? lane : 0);
-            const Slot4<S> od = W.sd[a];
-            const V3<S> u = {od.x, od.y, od.z};
-            V3<S> ul = vzero<S>();
-            if (L::nlo) {
-                const Slot4<S> ol = W.sl[a];
-                ul = {ol.x, ol.y, ol.z};
-            }
-            const S aa = od.w;
-            OwnAcc<S> acc;
-            acc.zero();
-
-            // evaluate own slot a against partner slot b; returns the partner's share
-            auto pair = [&](bool act, int b) -> PGrad<S> {
-                const Slot4<S> pd = W.sd[b];
-                const V3<S> v = {pd.x, pd.y, pd.z};
-                V3<S> vl = vzero<S>();
+        const unsigned int cnt0 = cnt;
+        using T = typename Traits<S>::T;
+        const float f_mid = (float)G.sqcut;
+        const double d_lo = G.sqcut - G.band64, d_hi = G.sqcut + G.band64;
+        // The pair loops.  FAST (items that do not wrap): one compare with cutoff^2 decides every
+        // third edge, and `amb` records whether one fell inside the guard band, where the compare
+        // may differ from the reference's test.  Outside the band both decide alike, so an item
+        // without such an edge has exactly the results of the exact form.
+        auto sweep = [&](auto fast_tag) -> bool {
+            constexpr bool FAST = decltype(fast_tag)::value;
+            bool amb = false;
+            for (int A0 = 0; A0 < mI; A0 += 32) {
+                const int mA = min(32, mI - A0);
+                const bool own = lane < mA;
+                const int a = A0 + (own ? lane : 0);
+                const Slot4<S> od = W.sd[a];
+                const V3<S> u = {od.x, od.y, od.z};
+                V3<S> ul = vzero<S>();
                 if (L::nlo) {
-                    const Slot4<S> pl = W.sl[b];
-                    vl = {pl.x, pl.y, pl.z};
+                    const Slot4<S> ol = W.sl[a];
+                    ul = {ol.x, ol.y, ol.z};
                 }
-                const V3<S> wv = third_edge(u, ul, v, vl);
-                const S cww = dot3(wv, wv);
-                bool inside = false;
-                if (act) inside = cut_inside(W, cb, G, a, b, wv, cww, rawok, sq_lo, sq_hi, Lx, Ly, Lz);
-                cnt += inside ? 1u : 0u;
-                const ATCoef<S> cf =
-                    at_coef<ENERGY>(aa, pd.w, cww, dot3(u, v), dot3(u, wv), dot3(v, wv), nu, nu3, nu15, inside, en);
-                acc.add(cf, u, wv);
-                return make_pgrad(cf, v, wv);
-            };
+                const S aa = od.w;
+                OwnAcc<S> acc;
+                acc.zero();
 
-            if (mJ == 0) {
-                // pairs inside block A: circular diagonals; y = (lane + d) mod mA advances by one per
-                // diagonal (lanes past the block cycle through valid slots and are masked)
-                int y = own ? lane : 0;
-                for (int d = 1; 2 * d <= mA; ++d) {
-                    y = y + 1 == mA ? 0 : y + 1;
-                    const bool act = own && (2 * d < mA || lane < d);
-                    const int b = A0 + y;
-                    const PGrad<S> gb = pair(act, b);
-                    if (act) pgrad_add(W.gr[b], gb);
-                    __syncwarp();
-                }
-            }
-            // pairs A x B with every later block B (of the same chunk, or of the second chunk)
-            for (int B0 = (mJ == 0 ? A0 + 32 : mI); B0 < Ms; B0 += 32) {
-                const int mB = min(32, Ms - B0);
-                if (mB >= 24) {
-                    for (int t = 0; t < 32; ++t) {
-                        const int y = (lane + t) & 31;
-                        const bool act = own && y < mB;
-                        const int b = B0 + (y < mB ? y : 0);
+                // evaluate own slot a against partner slot b; returns the partner's share
+                auto pair = [&](bool act, int b) -> PGrad<S> {
+                    const Slot4<S> pd = W.sd[b];
+                    const V3<S> v = {pd.x, pd.y, pd.z};
+                    V3<S> vl = vzero<S>();
+                    if (L::nlo) {
+                        const Slot4<S> pl = W.sl[b];
+                        vl = {pl.x, pl.y, pl.z};
+                    }
+                    const V3<S> wv = third_edge(u, ul, v, vl);
+                    const S cww = dot3(wv, wv);
+                    bool inside = false;
+                    if constexpr (FAST) {
+                        if constexpr (std::is_same<T, float>::value) {
+                            const float d2 = to_float(cww);
+                            inside = act && d2 <= f_mid;
+                            amb = amb || (act && d2 > sq_lo && d2 <= sq_hi);
+                        } else {
+                            const double d2 = to_double(cww);
+                            inside = act && d2 <= G.sqcut;
+                            amb = amb || (act && d2 > d_lo && d2 <= d_hi);
+                        }
+                    } else {
+                        if (act) inside = cut_inside(W, cb, G, a, b, wv, cww, rawok, sq_lo, sq_hi, Lx, Ly, Lz);
+                    }
+                    cnt += inside ? 1u : 0u;
+                    const ATCoef<S> cf =
+                        at_coef<ENERGY>(aa, pd.w, cww, dot3(u, v), dot3(u, wv), dot3(v, wv), nu, nu3, nu15, inside, en);
+                    acc.add(cf, u, wv);
+                    return make_pgrad(cf, v, wv);
+                };
+
+                if (mJ == 0) {
+                    // pairs inside block A: circular diagonals; y = (lane + d) mod mA advances by one per
+                    // diagonal (lanes past the block cycle through valid slots and are masked)
+                    int y = own ? lane : 0;
+                    for (int d = 1; 2 * d <= mA; ++d) {
+                        y = y + 1 == mA ? 0 : y + 1;
+                        const bool act = own && (2 * d < mA || lane < d);
+                        const int b = A0 + y;
                         const PGrad<S> gb = pair(act, b);
                         if (act) pgrad_add(W.gr[b], gb);
                         __syncwarp();
                     }
-                } else {
-                    for (int y = 0; y < mB; ++y) {
-                        const int b = B0 + y;
-                        pgrad_add_warp(W.gr[b], pair(own, b), lane);
-                        __syncwarp();
+                }
+                // pairs A x B with every later block B (of the same chunk, or of the second chunk)
+                for (int B0 = (mJ == 0 ? A0 + 32 : mI); B0 < Ms; B0 += 32) {
+                    const int mB = min(32, Ms - B0);
+                    if (mB >= 24) {
+                        for (int t = 0; t < 32; ++t) {
+                            const int y = (lane + t) & 31;
+                            const bool act = own && y < mB;
+                            const int b = B0 + (y < mB ? y : 0);
+                            const PGrad<S> gb = pair(act, b);
+                            if (act) pgrad_add(W.gr[b], gb);
+                            __syncwarp();
+                        }
+                    } else {
+                        for (int y = 0; y < mB; ++y) {
+                            const int b = B0 + y;
+                            pgrad_add_warp(W.gr[b], pair(own, b), lane);
+                            __syncwarp();
+                        }
                     }
                 }
+                // merge the own accumulator into its slot
+                if (own) acc.merge(W.gr[a]);
+                __syncwarp();
             }
-            // merge the own accumulator into its slot
-            if (own) acc.merge(W.gr[a]);
+            return amb;
+        };
+        bool exact_form = !rawok;
+        if (rawok && __any_sync(0xffffffffu, sweep(std::true_type{}))) {
+            // a third edge inside the guard band: drop the item's partial sums and run it again
+            // with the exact test
+            cnt = cnt0;
+            en = szero<S>();
+            for (int e = lane; e < Ms; e += 32) W.gr[e] = grad_zero<S>();
             __syncwarp();
+            exact_form = true;
         }
+        if (exact_form) sweep(std::false_type{});
 
         // flush the slots; s's gradient is minus the sum of all slot gradients
         V3<Acc> gia = widen(vzero<S>());
