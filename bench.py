@@ -505,14 +505,8 @@ def run_batch(args, local):
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    rng = np.random.default_rng(926762934)
-    systems = []
-    for i in range(64):
-        n = int(rng.integers(512, 4097))
-        side = generators.box_for_density(n, 2.048)
-        systems.append(generators.uniform(n, (side,) * 3, seed0=926762934 + i))
-    offsets = np.cumsum([0] + [len(st["x"]) for st in systems]).astype(np.int64)
-    cat = {k: np.concatenate([st[k] for st in systems]) for k in ("x", "y", "z")}
+    systems = generators.batch_of_systems(64, 512, 4096, 2.048)
+    offsets, cat = generators.pack_systems(systems)
 
     def timed(fn, reps):
         out = None

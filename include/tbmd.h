@@ -39,7 +39,7 @@ typedef enum {
     TBMD_NOT_READY = 3,       /* no particles set */
     TBMD_CAPACITY_RETRY = 4,  /* neighbour capacity still too small after the automatic retries */
     TBMD_CUDA_ERROR = 5,      /* a CUDA runtime call failed; see tbmd_last_error */
-    TBMD_TIMEOUT = 6,         /* a bounded device-side wait gave up (the kernel returned early) */
+    TBMD_TIMEOUT = 6,         /* reserved; never returned (no kernel of this path waits on another) */
     TBMD_NO_DEVICE = 7,       /* no CUDA device, or not an sm_100 device */
     TBMD_TOO_LARGE = 8,       /* n above the limit of an allocation-free entry point */
     TBMD_RANK_LAYOUT = 9      /* the reference's run on that many MPI ranks would stop (tbmd_rank_layout_of) */
@@ -216,9 +216,13 @@ int32_t tbmd_phase_times(const tbmd_ctx *ctx, double *ms, uint64_t *calls, uint6
  * about 3 MiB inside the library (held on every GPU that loads it until exit).  It computes the
  * stored forces (+grad E, no cutoff, strength nu) of all C(n,3) triplets with the NATA kernel in
  * FP64 or mixed precision on `stream` (cudaStream_t, NULL = legacy default stream), asynchronously.
- * 1 <= n <= TBMD_NOALLOC_MAX_N; larger n returns TBMD_TOO_LARGE without launching anything.  The
- * first call on a device looks up the scratch address (make it before any stream capture).  All
- * calls share the scratch, so calls that overlap on the GPU race and must be serialised. */
+ * 1 <= n <= TBMD_NOALLOC_MAX_N; larger n returns TBMD_TOO_LARGE without launching anything; a
+ * non-finite nu returns TBMD_INVALID_ARG.  The first call on a device looks up the scratch address
+ * in the context current at that time and caches it with that context's unique id; a call made
+ * while another context is current (after cudaDeviceReset, or a context the caller created) looks
+ * it up again.  Make the first call, and the first one after such a change, before any stream
+ * capture.  All calls share the scratch, so calls that overlap on the GPU race and must be
+ * serialised. */
 #define TBMD_NOALLOC_MAX_N 4096
 tbmd_status tbmd_nata_forces_noalloc(int64_t n, const double *x, const double *y, const double *z, double nu,
                                      int32_t precision, double *fx, double *fy, double *fz, void *stream);

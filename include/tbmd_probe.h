@@ -15,7 +15,8 @@ extern "C" {
 #endif
 
 /* Measured FMA throughput of `device` in TFLOP/s (an FMA counts 2 FLOP): fp64 = 0 for the FP32
- * pipe, 1 for the FP64 pipe.  Runs about 0.1-0.3 s; returns a negative value on a CUDA error. */
+ * pipe, 1 for the FP64 pipe.  Runs about 0.1-0.3 s; returns a negative value on a CUDA error.  The
+ * calling thread's current device is the same afterwards. */
 double tbmd_probe_fma_tflops(int32_t device, int32_t fp64);
 
 #ifdef __cplusplus

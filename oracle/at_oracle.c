@@ -370,6 +370,61 @@ uint64_t tbo_forces_cells(int64_t n, const double *x, const double *y, const dou
     return total;
 }
 
+/* Stored force (+grad E) on each of the nsel particles sel[] from every triplet that contains it,
+ * with no cutoff: NATA's view of one particle (NATA.cpp:27-55 sums, for particle i, the triplets
+ * it takes part in).  Each triplet {p, j, k} is evaluated with the reference's arithmetic in its
+ * sorted order a < b < c (at_triplet, AxilrodTeller.cpp:23-129), and p's share is the amount the
+ * reference subtracts for p's role; the three roles are summed like SumUpParticles
+ * (Algorithm.cpp:245-248): f = f0 + (f1 + f2).  O(n^2) per particle, so the C(n,3) force of a few
+ * particles of a large system can be pinned without the whole O(n^3) loop.  Threads split the j
+ * loop; their partial sums are added in thread order. */
+void tbo_forces_selected(int64_t n, const double *x, const double *y, const double *z, double nu,
+                         const int64_t *sel, int64_t nsel, double *fx, double *fy, double *fz, int nthreads)
+{
+    nthreads = clamp_threads(nthreads);
+    double *part = (double *)calloc((size_t)(9 * nthreads), sizeof(double));
+    if (!part) return;
+    for (int64_t s = 0; s < nsel; ++s) {
+        const int64_t p = sel[s];
+        memset(part, 0, sizeof(double) * 9 * (size_t)nthreads);
+#pragma omp parallel num_threads(nthreads)
+        {
+            double *acc = part + 9 * omp_get_thread_num(); /* [role][xyz] */
+#pragma omp for schedule(dynamic, 8)
+            for (int64_t j = 0; j < n; ++j) {
+                if (j == p) continue;
+                for (int64_t k = j + 1; k < n; ++k) {
+                    if (k == p) continue;
+                    int64_t a = p, b = j, c = k; /* sort into a < b < c, remembering p's role */
+                    int role;
+                    if (p < j) {
+                        role = 0;
+                    } else if (p < k) {
+                        a = j;
+                        b = p;
+                        role = 1;
+                    } else {
+                        a = j;
+                        b = k;
+                        c = p;
+                        role = 2;
+                    }
+                    double ci[3], cj[3], ck[3];
+                    at_triplet(nu, x[a], y[a], z[a], x[b], y[b], z[b], x[c], y[c], z[c], ci, cj, ck);
+                    const double *cp = role == 0 ? ci : (role == 1 ? cj : ck);
+                    for (int d = 0; d < 3; ++d) acc[3 * role + d] -= cp[d];
+                }
+            }
+        }
+        for (int t = 1; t < nthreads; ++t)
+            for (int q = 0; q < 9; ++q) part[q] += part[9 * t + q];
+        fx[s] = part[0] + (part[3] + part[6]);
+        fy[s] = part[1] + (part[4] + part[7]);
+        fz[s] = part[2] + (part[5] + part[8]);
+    }
+    free(part);
+}
+
 /* Triplet energy from dot products: u = xj - xi, v = xk - xi, w = xk - xj,
  * cos_i cos_j cos_k = -(u.v)(u.w)(v.w) / (|u|^2 |v|^2 |w|^2). */
 /* scale = 0: the triplet energy nu (1 + 3 cos cos cos) / (r1 r2 r3)^3.

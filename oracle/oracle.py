@@ -15,8 +15,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "liboracle.so"
 REF_DIR = HERE / "_ref"
-# where the reference's sources are read when present (the build container only)
-REFERENCE_ROOT = Path("/root/reference")
+# Where the reference's sources are read when present (the build machine only): the directory named
+# by TBMD_REFERENCE_ROOT, else a checkout named "reference" beside this repository.
+REFERENCE_ROOT = Path(os.environ.get("TBMD_REFERENCE_ROOT", str(HERE.parent.parent / "reference")))
 STUB_INCLUDE = HERE / "refstub" / "inc"  # stand-in mpi.h and Eigen/Dense for the reference's headers
 
 ALGORITHMS = {"nata": 0, "p3bca": 1, "auta": 2}
@@ -55,6 +56,9 @@ def lib():
         _lib.tbo_forces_bruteforce.restype = C.c_uint64
         _lib.tbo_forces_cells.argtypes = [i64, d, d, d, C.c_double, C.c_double, d, d, d, d, d, C.c_int]
         _lib.tbo_forces_cells.restype = C.c_uint64
+        _lib.tbo_forces_selected.argtypes = [i64, d, d, d, C.c_double, C.POINTER(C.c_int64), i64, d, d, d,
+                                             C.c_int]
+        _lib.tbo_forces_selected.restype = None
         _lib.tbo_cell_dims.argtypes = [d, C.c_double, C.POINTER(C.c_int), d]
         _lib.tbo_cell_assign.argtypes = [i64, d, d, d, C.c_double, d, d, C.POINTER(C.c_int),
                                          C.POINTER(C.c_int32)]
@@ -111,6 +115,18 @@ def forces(x, y, z, nu: float = 1.0, cutoff: float = -1.0, L=None, lo=None, nthr
     if c == 2**64 - 1:
         raise MemoryError("oracle allocation failed")
     return fx, fy, fz, int(c)
+
+
+def forces_selected(x, y, z, idx, nu: float = 1.0, nthreads: int = 0):
+    """Stored forces (+grad E, no cutoff) on the particles idx only, from every triplet containing
+    each (O(n^2) per particle, the reference's per-triplet arithmetic).  Returns (fx, fy, fz) of
+    len(idx)."""
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    sel = np.ascontiguousarray(idx, dtype=np.int64)
+    out = [np.zeros(len(sel)) for _ in range(3)]
+    lib().tbo_forces_selected(len(x), _p(x), _p(y), _p(z), nu, sel.ctypes.data_as(C.POINTER(C.c_int64)), len(sel),
+                              *[_p(o) for o in out], nthreads)
+    return tuple(out)
 
 
 def cell_dims(L, cutoff):

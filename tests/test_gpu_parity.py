@@ -150,6 +150,15 @@ def test_c2_n8192_nata_auta_fp64_mixed():
     # sum |E_t| over 9.2e10 triplets is too costly for the oracle here; for a uniform system it is
     # within a few percent of |E|, so the bound is taken against |E| with a 5x margin
     assert abs(ea - en) <= 1e-12 * abs(ea) and abs(em - ea) <= 5 * MIXED_ENERGY_TOL * abs(ea)
+    # against the oracle: 64 seeded random particles, each with the force of all C(8191, 2) triplets
+    # it belongs to, in the reference's per-triplet arithmetic (NATA's view of one particle)
+    idx = np.sort(np.random.default_rng(8192).choice(8192, 64, replace=False))
+    ref = np.stack(O.forces_selected(st["x"], st["y"], st["z"], idx, 1.0, nthreads=0), 1)
+    for f, tol, what in ((fa, FP64_TOL, "auta fp64"), (fn, FP64_TOL, "nata fp64"), (fm, MIXED_FORCE_TOL, "auta mixed"),
+                         (fnm, MIXED_FORCE_TOL, "nata mixed")):
+        assert rel_l2(f[idx], ref) <= tol, (what, rel_l2(f[idx], ref))
+        # and particle by particle, against the largest force of the sample
+        assert np.abs(f[idx] - ref).max() <= 10 * tol * np.abs(ref).max(), what
 
 
 @pytest.mark.parametrize("cutoff", [2.0, 1.5])

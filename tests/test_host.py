@@ -89,6 +89,23 @@ def test_cli_errors_like_reference():
         assert r.returncode == 1 and "Help:" in r.stdout, bad
 
 
+REF_MAIN = ROOT / "oracle" / "_ref" / "ref_main"
+
+
+@pytest.mark.skipif(not (MAIN.exists() and REF_MAIN.exists()), reason="tbmd_main or the reference build absent")
+def test_cli_help_is_the_references():
+    """A flag without its value prints the help and exits 1 in both programs (cli.hpp:54-58).  The
+    reference's 15 help lines (cli.hpp:27-45, its "-gx,--gravityZ" label included) come out byte for
+    byte; this build's own options follow them."""
+    ref = subprocess.run([str(REF_MAIN), "-c"], capture_output=True)
+    mine = subprocess.run([str(MAIN), "-c"], capture_output=True)
+    assert ref.returncode == 1 and mine.returncode == 1
+    ref_lines = ref.stdout.split(b"\n")
+    assert len(ref_lines) == 16 and ref_lines[-1] == b""
+    assert mine.stdout.split(b"\n")[:15] == ref_lines[:15]
+    assert b"GPU options:" in mine.stdout
+
+
 @pytest.mark.skipif(not MAIN.exists(), reason="tbmd_main not built")
 def test_cli_missing_input_fails():
     r = subprocess.run([str(MAIN), "-csv", "/nonexistent.csv", "-i", "1"], capture_output=True, text=True)

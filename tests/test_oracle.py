@@ -87,3 +87,13 @@ def test_cell_assignment_wraps_periodically():
     assert dims == (4, 4, 4)
     cx = cell % dims[0]
     assert cx.tolist() == [0, 3, 3, 0, 2]
+
+
+def test_selected_forces_equal_the_reference_run():
+    """forces_selected (one particle's triplets, O(n^2)) against the reference's own forces on the
+    N=1000 fixture: the same per-triplet arithmetic, summed in another order."""
+    inp, out, _, _ = G.load("tests_fixture_n1000_auta")
+    idx = np.array([0, 1, 499, 998, 999, 321])
+    got = np.stack(O.forces_selected(inp["x"], inp["y"], inp["z"], idx, 1.0, nthreads=4), 1)
+    ref = np.stack([out["fx"][idx], out["fy"][idx], out["fz"][idx]], 1)
+    assert np.linalg.norm(got - ref) <= 1e-13 * np.linalg.norm(ref)

@@ -62,6 +62,9 @@ struct Args {
     std::string tuneCache, dumpFull;
 };
 
+// The first 15 lines are the reference's help text byte for byte (cli.hpp:27-45), including its
+// "-gx,--gravityZ" label (the parser itself accepts --gravityX, as the reference's does), so that
+// scripts that read the reference's output read this one too.  This build's own options follow.
 void printHelp()
 {
     std::cout << "Help: \n"
@@ -70,16 +73,17 @@ void printHelp()
               << "\t-a,--algorithm\t\talgorithm to use (\"nata\", \"p3bca\", \"auta\")\n"
               << "\t-i,--iterations\t\tnum of iterations to simulate\n"
               << "\t-d,--delta\t\tduration of one simulation step\n"
-              << "\t-gx,--gravityX\t\tgravitational force in x-direction\n"
+              << "\t-gx,--gravityZ\t\tgravitational force in x-direction\n"
               << "\t-gy,--gravityY\t\tgravitational force in y-direction\n"
               << "\t-gz,--gravityZ\t\tgravitational force in z-direction\n"
               << "\t-csv,--csv\t\tcsv file with particles\n"
               << "\t-o,--out\t\tcsv base file name that will be used to create all csv outputs from each "
                  "simulation step\n"
               << "-op,--outProfile\t\tjson file to save profile output\n"
-              << "-decomp,--decomp\t\t(optimal | naive) decomposition strategy for cart topology (with -np)\n"
-              << "-benchyaml,--benchyaml\t\tYAML file that contains config for benchmarks (ignored)\n"
+              << "-decomp,--decomp\t\t(optimal | naive) decomposition strategy for cart topology\n"
+              << "-benchyaml,--benchyaml\t\tYAML file that contains config for benchmarks\n"
               << "\t-c,--cutoff\t\tcutoff distance\n"
+              << "Notes: -decomp applies with -np; -benchyaml is accepted and ignored.\n"
               << "GPU options:\n"
               << "\t-prec\t\tfp64 | mixed\n\t-nu\t\tAT strength (1.0)\n\t-device\t\tCUDA device\n"
               << "\t-nograph\t\tno CUDA graph\n\t-tune\t\tautotuner cache file\n"

@@ -26,35 +26,49 @@ __global__ void __launch_bounds__(256) k_fma(T *out, int iters, T a, T b)
 }
 
 template <class T>
-double run(int device)
+double run_on_current(int device)
 {
-    if (cudaSetDevice(device) != cudaSuccess) return -1.0;
     int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms < 1) return -1.0;
     const int blocks = sms * 8, threads = 256, iters = sizeof(T) == 8 ? 4096 : 8192;
     T *out = nullptr;
     if (cudaMalloc(&out, sizeof(T) * blocks * threads) != cudaSuccess) return -1.0;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    k_fma<T><<<blocks, threads>>>(out, iters, T(0.999999), T(1e-7));  // warm-up
-    float best = 1e30f;
-    for (int rep = 0; rep < 5; ++rep) {
-        cudaEventRecord(e0);
-        k_fma<T><<<blocks, threads>>>(out, iters, T(0.999999), T(1e-7));
-        cudaEventRecord(e1);
-        cudaEventSynchronize(e1);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best) best = ms;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    double result = -1.0;
+    if (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
+        k_fma<T><<<blocks, threads>>>(out, iters, T(0.999999), T(1e-7));  // warm-up
+        float best = 1e30f;
+        bool ok = cudaGetLastError() == cudaSuccess;
+        for (int rep = 0; ok && rep < 5; ++rep) {
+            ok = cudaEventRecord(e0) == cudaSuccess;
+            k_fma<T><<<blocks, threads>>>(out, iters, T(0.999999), T(1e-7));
+            ok = ok && cudaGetLastError() == cudaSuccess && cudaEventRecord(e1) == cudaSuccess &&
+                 cudaEventSynchronize(e1) == cudaSuccess;
+            float ms = 0;
+            ok = ok && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+            if (ok && ms < best) best = ms;
+        }
+        if (ok && best > 0.f && best < 1e30f) {
+            const double flops = 2.0 * 8.0 * (double)iters * blocks * threads;
+            result = flops / (best * 1e-3) / 1e12;
+        }
     }
-    cudaError_t err = cudaGetLastError();
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
     cudaFree(out);
-    if (err != cudaSuccess) return -1.0;
-    const double flops = 2.0 * 8.0 * (double)iters * blocks * threads;
-    return flops / (best * 1e-3) / 1e12;
+    return result;
+}
+
+// Runs on `device` and leaves the caller's current device as it was.
+template <class T>
+double run(int device)
+{
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess) return -1.0;
+    if (cudaSetDevice(device) != cudaSuccess) return -1.0;
+    const double r = run_on_current<T>(device);
+    if (cudaSetDevice(prev) != cudaSuccess) return -1.0;
+    return r;
 }
 
 }  // namespace

@@ -126,3 +126,25 @@ def as_csv_values(st: dict) -> dict:
 def box_for_density(n: int, density: float = 2.048) -> float:
     """Cube side with n / side^3 = density (131072 at 2.048 gives 40.0)."""
     return (n / density) ** (1.0 / 3.0)
+
+
+def batch_of_systems(count: int = 64, nmin: int = 512, nmax: int = 4096, density: float = 2.048,
+                     seed: int = SEED0) -> list:
+    """Independent systems for the batched path: system i has N_i drawn uniformly from nmin..nmax
+    (numpy's default generator seeded with `seed`) and is uniform in a cube scaled to `density`,
+    drawn like UniformGenerator with seed0 = seed + i.  With the defaults this is the 64-system
+    workload of the batched benchmark."""
+    rng = np.random.default_rng(seed)
+    systems = []
+    for i in range(count):
+        n = int(rng.integers(nmin, nmax + 1))
+        side = box_for_density(n, density)
+        systems.append(uniform(n, (side,) * 3, seed0=seed + i))
+    return systems
+
+
+def pack_systems(systems: list):
+    """Concatenate systems back to back: (offsets[count + 1], {'x','y','z'} arrays)."""
+    offsets = np.cumsum([0] + [len(s["x"]) for s in systems]).astype(np.int64)
+    cat = {k: np.concatenate([s[k] for s in systems]) for k in ("x", "y", "z")}
+    return offsets, cat
