@@ -152,7 +152,8 @@ __device__ __forceinline__ double dual_tangent(Dual<double> a) { return a.d; }
 // mixed form (S = float) the rounding remainder is kept as a second float ("lo"), so that the third
 // edge w = v - u = (v_hi - u_hi) + (v_lo - u_lo) is accurate to a relative FP32 epsilon even when
 // j and k are close to each other and far from i (v_hi - u_hi is then exact by Sterbenz's lemma).
-// For double and the dual types the lo part is identically zero and compiled away.
+// The mixed adjoint (Dual<float>) splits the value the same way.  For double and Dual<double> the lo
+// part is identically zero and compiled away.
 
 template <class S>
 struct HasLo {
@@ -160,6 +161,12 @@ struct HasLo {
 };
 template <>
 struct HasLo<float> {
+    static constexpr bool value = true;
+};
+// The mixed adjoint keeps the lo part of the value too (its tangent needs none: a tangent is a
+// difference of cotangents, which do not nearly cancel the way two close edges from i do).
+template <>
+struct HasLo<Dual<float>> {
     static constexpr bool value = true;
 };
 
@@ -175,6 +182,12 @@ __device__ __forceinline__ void split<float>(double d, double, float &hi, float 
 {
     hi = (float)d;
     lo = (float)(d - (double)hi);
+}
+template <>
+__device__ __forceinline__ void split<Dual<float>>(double d, double t, Dual<float> &hi, Dual<float> &lo)
+{
+    hi = {(float)d, (float)t};
+    lo = {(float)(d - (double)hi.v), 0.f};
 }
 
 template <class S>

@@ -55,6 +55,17 @@ struct Tile<float> {
         lz = l.z;
     }
 };
+template <>
+struct Tile<Dual<float>> {
+    Dual<float> vx, vy, vz, b, lx, ly, lz, pad;
+    __device__ __forceinline__ V3<Dual<float>> lo() const { return {lx, ly, lz}; }
+    __device__ __forceinline__ void set_lo(V3<Dual<float>> l)
+    {
+        lx = l.x;
+        ly = l.y;
+        lz = l.z;
+    }
+};
 
 template <class S>
 __device__ __forceinline__ V3<typename Traits<S>::Acc> widen(V3<S> a)
@@ -1354,8 +1365,8 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
         }
         const bool rawok = G.raw_ok && __all_sync(0xffffffffu, nowrap);
         // FP32 thresholds: the narrow band of hi + lo edges that do not wrap (mixed forces), else
-        // the band of FP32 geometry with wrapping or without lo parts (the mixed adjoint)
-        const bool narrow = rawok && L::mixed;
+        // the band of FP32 geometry with wrapping (the mixed adjoint always keeps this wide band)
+        const bool narrow = rawok && std::is_same<S, float>::value;
         const float sq_lo = narrow ? G.raw_lo : (float)G.sqcut - G.band;
         const float sq_hi = narrow ? G.raw_hi : (float)G.sqcut + G.band;
         __syncwarp();
