@@ -152,8 +152,8 @@ __device__ __forceinline__ double dual_tangent(Dual<double> a) { return a.d; }
 // mixed form (S = float) the rounding remainder is kept as a second float ("lo"), so that the third
 // edge w = v - u = (v_hi - u_hi) + (v_lo - u_lo) is accurate to a relative FP32 epsilon even when
 // j and k are close to each other and far from i (v_hi - u_hi is then exact by Sterbenz's lemma).
-// The mixed adjoint (Dual<float>) splits the value the same way.  For double and Dual<double> the lo
-// part is identically zero and compiled away.
+// The mixed adjoint (Dual<float>) splits the value and its tangent the same way.  For double and
+// Dual<double> the lo part is identically zero and compiled away.
 
 template <class S>
 struct HasLo {
@@ -163,8 +163,7 @@ template <>
 struct HasLo<float> {
     static constexpr bool value = true;
 };
-// The mixed adjoint keeps the lo part of the value too (its tangent needs none: a tangent is a
-// difference of cotangents, which do not nearly cancel the way two close edges from i do).
+// The mixed adjoint splits the value and the tangent into hi + lo parts too (see dot_uv).
 template <>
 struct HasLo<Dual<float>> {
     static constexpr bool value = true;
@@ -187,7 +186,7 @@ template <>
 __device__ __forceinline__ void split<Dual<float>>(double d, double t, Dual<float> &hi, Dual<float> &lo)
 {
     hi = {(float)d, (float)t};
-    lo = {(float)(d - (double)hi.v), 0.f};
+    lo = {(float)(d - (double)hi.v), (float)(t - (double)hi.d)};
 }
 
 template <class S>
@@ -195,6 +194,30 @@ __device__ __forceinline__ V3<S> third_edge(V3<S> uh, V3<S> ul, V3<S> vh, V3<S> 
 {
     if (HasLo<S>::value) return (vh - uh) + (vl - ul);
     return vh - uh;
+}
+
+// p = u.v of the triplet math, from the edges u, v from i (hi and lo parts) and the third edge w.
+// For the mixed adjoint the tangent u'.v + u.v' is formed as u'.w + (u' + v').u (v = u + w): for a
+// close pair j, k with large, nearly opposite cotangents (a force-matching cotangent of a close pair
+// is one), u' and v' nearly cancel, and u'.v + u.v' in FP32 would lose about log2(|u| / |w|) bits.
+// u' + v' is summed from the hi and the lo parts of both tangents (the hi sum is exact where they
+// cancel), so every term left is free of cancellation.
+template <class S>
+__device__ __forceinline__ S dot_uv(V3<S> uh, V3<S>, V3<S> vh, V3<S>, V3<S>)
+{
+    return dot3(uh, vh);
+}
+template <>
+__device__ __forceinline__ Dual<float> dot_uv<Dual<float>>(V3<Dual<float>> uh, V3<Dual<float>> ul, V3<Dual<float>> vh,
+                                                          V3<Dual<float>> vl, V3<Dual<float>> w)
+{
+    const float val = fmaf(uh.x.v, vh.x.v, fmaf(uh.y.v, vh.y.v, uh.z.v * vh.z.v));
+    const float sx = (uh.x.d + vh.x.d) + (ul.x.d + vl.x.d);
+    const float sy = (uh.y.d + vh.y.d) + (ul.y.d + vl.y.d);
+    const float sz = (uh.z.d + vh.z.d) + (ul.z.d + vl.z.d);
+    const float tan = fmaf(uh.x.d, w.x.v, fmaf(uh.y.d, w.y.v, uh.z.d * w.z.v)) +
+                      fmaf(sx, uh.x.v, fmaf(sy, uh.y.v, sz * uh.z.v));
+    return {val, tan};
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -234,6 +257,8 @@ struct Grid {
     float raw_lo;   // FP32 third-edge test without wrapping, hi + lo edges: d2 <= raw_lo is inside,
     float raw_hi;   // d2 > raw_hi outside, the exact test in between
     int raw_ok;     // every box length >= 4 cutoffs: raw distance = periodic formula for non-wrapping pairs
+    float hi_lo;    // FP32 test on the hi parts of edges that do not wrap (k_p3pair's adjacency):
+    float hi_hi;    //   d2 <= hi_lo inside, d2 > hi_hi outside, the exact test in between
 };
 
 // Several independent systems packed back to back: system s owns particles (and sorted slots)

@@ -118,7 +118,8 @@ __device__ __forceinline__ ATCoef<S> triplet(V3<S> uh, V3<S> ul, S a, V3<S> vh, 
                                              bool valid, S &e, V3<S> &w)
 {
     w = third_edge(uh, ul, vh, vl);
-    return at_coef<ENERGY>(a, b, dot3(w, w), dot3(uh, vh), dot3(uh, w), dot3(vh, w), nu, nu3, nu15, valid, e);
+    return at_coef<ENERGY>(a, b, dot3(w, w), dot_uv(uh, ul, vh, vl, w), dot3(uh, w), dot3(vh, w), nu, nu3, nu15,
+                           valid, e);
 }
 
 // Decode a sweep work item: block b with prefix[b] <= w < prefix[b+1], i = w - prefix[b].
@@ -357,7 +358,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_nata(int64_t n, Pos pos, double 
                     const V3<S> w = third_edge(u[r], ul[r], v, vl);
                     // basis (u, w) when |u| <= |v|, else (v, w): see at_self
                     const bool ub = to_float(aa[r]) <= to_float(e.b);
-                    const ATSelf<S> cf = at_self<ENERGY>(aa[r], e.b, dot3(w, w), dot3(u[r], v), dot3(u[r], w),
+                    const ATSelf<S> cf = at_self<ENERGY>(aa[r], e.b, dot3(w, w), dot_uv(u[r], ul[r], v, vl, w), dot3(u[r], w),
                                                          dot3(v, w), nu, nu3, nu15, valid, ub, e_r);
                     if (ENERGY && i < jj[r]) en = en + e_r;
                     if (ub)
@@ -1424,7 +1425,7 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
                     }
                     cnt += inside ? 1u : 0u;
                     const ATCoef<S> cf =
-                        at_coef<ENERGY>(aa, pd.w, cww, dot3(u, v), dot3(u, wv), dot3(v, wv), nu, nu3, nu15, inside, en);
+                        at_coef<ENERGY>(aa, pd.w, cww, dot_uv(u, ul, v, vl, wv), dot3(u, wv), dot3(v, wv), nu, nu3, nu15, inside, en);
                     acc.add(cf, u, wv);
                     return make_pgrad(cf, v, wv);
                 };
@@ -1523,6 +1524,8 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
     flush(cur_sys);
 }
 
+#include "p3bca_pairs.cuh"
+
 void fill_grid_test_params(Grid &g);
 
 // Half-width of the uncertainty band around cutoff^2 of the guarded third-edge test, for unit
@@ -1564,6 +1567,15 @@ static int raw_test_ok(const Grid &g)
 // band of the wrapped form, whose L - |d| carries errors of order 2^-24 L.
 static double raw_band(const Grid &g) { return 36.0 / 16777216.0 * g.sqcut; }  // 2^-24
 
+// Half-width of the band of the FP32 adjacency test of k_p3pair on the hi parts alone of edges that
+// do not wrap (each component within the cutoff c of s).  hi = fl32(e) differs from the FP64 edge e
+// by at most 2^-24 |e_i| per component, so a component of w = hi_q - hi_p, rounded once more, is
+// within 2^-24 (|e_p,i| + |e_q,i| + |w_i|) <= 4 * 2^-24 c of the reference's x_q - x_p (|w| <= 2 c).
+// The squared length then differs from the reference's by at most 8 sqrt(3) 2^-24 c |w| (about
+// 13.9 * 2^-24 c^2 near the cutoff), plus 3 * 2^-24 c^2 from its own three roundings and 2^-24 c^2
+// from rounding the thresholds: 18 * 2^-24 c^2.  Four times that is used.
+static double hi_band(const Grid &g) { return 72.0 / 16777216.0 * g.sqcut; }
+
 void fill_grid_test_params(Grid &g)
 {
     g.band = (float)guard_band(g, 1.0 / 8388608.0);      // 2^-23
@@ -1571,6 +1583,28 @@ void fill_grid_test_params(Grid &g)
     g.raw_lo = (float)(g.sqcut - raw_band(g));
     g.raw_hi = (float)(g.sqcut + raw_band(g));
     g.raw_ok = raw_test_ok(g);
+    g.hi_lo = (float)(g.sqcut - hi_band(g));
+    g.hi_hi = (float)(g.sqcut + hi_band(g));
+}
+
+// The forces (FP32 and FP64 geometry, with or without the energy) run the pair-compacted k_p3pair;
+// the adjoint (dual types) runs k_p3bca.
+template <class S, bool ENERGY>
+static auto p3_kernel()
+{
+    if constexpr (Traits<S>::dual)
+        return k_p3bca<S, ENERGY>;
+    else
+        return k_p3pair<S, ENERGY>;
+}
+
+template <class S>
+static size_t p3_warp_bytes()
+{
+    if constexpr (Traits<S>::dual)
+        return (size_t)2 * P3_CHUNK * SlotLayout<S>::bytes_per_slot;
+    else
+        return PairLayout<S>::bytes;
 }
 
 template <class S>
@@ -1581,13 +1615,14 @@ static cudaError_t plan_p3bca_t(bool energy, int cap, int warps, P3Plan *plan)
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     (void)cap;
-    const size_t per_warp = (size_t)2 * P3_CHUNK * SlotLayout<S>::bytes_per_slot;
-    const size_t smem_cap = 200 * 1024;
+    const size_t per_warp = p3_warp_bytes<S>();
+    const size_t smem_cap = 220 * 1024;
     if (warps < 1) warps = 1;
+    if (warps > 8) warps = 8;
     while (warps > 1 && per_warp * warps > smem_cap) --warps;
     if (per_warp * warps > smem_cap) return cudaErrorInvalidValue;
     const size_t smem = per_warp * warps;
-    auto kern = energy ? k_p3bca<S, true> : k_p3bca<S, false>;
+    auto kern = energy ? p3_kernel<S, true>() : p3_kernel<S, false>();
     if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
         return e;
     int per_sm = 0;
@@ -1619,10 +1654,8 @@ static cudaError_t launch_p3bca_t(bool energy, int64_t n, const Grid &g, const G
 {
     cudaError_t e;
     if ((e = cudaMemsetAsync(cb.work_counter, 0, 2 * sizeof(unsigned int), st)) != cudaSuccess) return e;
-    if (energy)
-        k_p3bca<S, true><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, set, cb, nu, eo, co);
-    else
-        k_p3bca<S, false><<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, set, cb, nu, eo, co);
+    auto kern = energy ? p3_kernel<S, true>() : p3_kernel<S, false>();
+    kern<<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, set, cb, nu, eo, co);
     return cudaGetLastError();
 }
 
