@@ -227,6 +227,16 @@ int32_t tbmd_phase_times(const tbmd_ctx *ctx, double *ms, uint64_t *calls, uint6
 tbmd_status tbmd_nata_forces_noalloc(int64_t n, const double *x, const double *y, const double *z, double nu,
                                      int32_t precision, double *fx, double *fy, double *fz, void *stream);
 
+/* Debug-build index checks.  No counterpart in the reference (its debug aid would be a
+ * compute-sanitizer run).  A library built with -DTBMD_BOUNDS_CHECK (python -m
+ * threebodymdalgorithms_b200.build --bounds-check, libtbmd_checked.so) checks the computed indices of
+ * its kernels (cells, sorted slots, neighbour lists, staged slots, pair places, sweep items): an
+ * index outside its array is recorded on the device and replaced by 0, so the kernel neither faults
+ * nor traps.  This call waits for the device, writes the number of violations since the last call
+ * (-1 if the device could not be read) and the site, index and array size of the first one, clears
+ * the record and returns 1 for a checked build; a normal build records nothing and returns 0. */
+int32_t tbmd_bounds_report(int64_t *violations, int32_t *site, int64_t *index, int64_t *size);
+
 /* Layout of the reference's run on P MPI ranks (host only, no device work).  Results do not depend
  * on P: every rank layout evaluates each triplet once, and the GPU evaluates them all in one
  * process.  What P decides in the reference is the process grid and whether the run starts, and

@@ -71,3 +71,23 @@ def test_no_device_is_a_loud_error():
     with pytest.raises(_lib.TbmdError) as e:
         _lib.Context("auta")
     assert e.value.status == 7
+
+
+CHECKED = Path(_lib.__file__).resolve().parent / "libtbmd_checked.so"
+
+
+def test_bounds_report_of_the_normal_build_records_nothing():
+    """The normal build has no index checks: tbmd_bounds_report returns 0 (no device needed to ask)."""
+    lib = _lib.load()
+    v, site = C.c_int64(), C.c_int32()
+    if _lib.LIB_PATH.name == "libtbmd.so":
+        assert lib.tbmd_bounds_report(C.byref(v), C.byref(site), None, None) == 0
+
+
+@pytest.mark.skipif(not CHECKED.exists(), reason="bounds-checked build not made (build --bounds-check)")
+def test_checked_build_exports_the_same_symbols():
+    lib = C.CDLL(str(CHECKED))
+    for name in all_declared():
+        assert hasattr(lib, name), name
+    v = C.c_int64()
+    assert lib.tbmd_bounds_report(C.byref(v), None, None, None) == 1

@@ -3,11 +3,13 @@ library; there is no CPU fallback.  Loading fails loudly if the library is missi
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
 
-LIB_PATH = Path(__file__).resolve().parent / "libtbmd.so"
+# TBMD_LIBRARY selects another build of the library, e.g. the bounds-checked libtbmd_checked.so
+LIB_PATH = Path(os.environ.get("TBMD_LIBRARY") or Path(__file__).resolve().parent / "libtbmd.so")
 
 NATA, P3BCA, AUTA = 0, 1, 2
 FP64, MIXED = 0, 1
@@ -24,6 +26,7 @@ EXPORTS = ("tbmd_config_init", "tbmd_create", "tbmd_destroy", "tbmd_last_error",
            "tbmd_forces", "tbmd_adjoint", "tbmd_forces_device", "tbmd_adjoint_device", "tbmd_set_domain",
            "tbmd_cells", "tbmd_batch_forces", "tbmd_batch_adjoint", "tbmd_autotune", "tbmd_tuning", "tbmd_sync",
            "tbmd_kernel_launches", "tbmd_set_profiling", "tbmd_phase_times", "tbmd_nata_forces_noalloc",
+           "tbmd_bounds_report",
            "tbmd_generator_init", "tbmd_generate_particles", "tbmd_rank_layout_of", "tbmd_step_host")
 PHASES = ("predictor", "cells", "neighbors", "triplets", "update")
 
@@ -58,6 +61,16 @@ class RankLayout(C.Structure):
                 ("cell_size", C.c_double * 3), ("particles_per_rank", C.c_int64), ("dummies", C.c_int64)]
 
 _lib = None
+
+
+def bounds_report():
+    """Index checks of a bounds-checked build (libtbmd_checked.so): (checked, violations, site, index,
+    size) of the first index found outside its array since the last report; checked is False for the
+    normal build, which records nothing.  Waits for the device."""
+    lib = load()
+    v, site, idx, size = C.c_int64(), C.c_int32(), C.c_int64(), C.c_int64()
+    checked = lib.tbmd_bounds_report(C.byref(v), C.byref(site), C.byref(idx), C.byref(size))
+    return bool(checked), v.value, site.value, idx.value, size.value
 
 
 def load():
@@ -101,6 +114,7 @@ def load():
         "tbmd_rank_layout_of": (C.c_int, [i32, i32, i32, C.c_double, d, i64, C.POINTER(RankLayout), C.c_char_p,
                                           i32]),
         "tbmd_step_host": (C.c_int, [vp, i64, pi32] + [d] * 10 + [i32, pu64, pi32] + [d] * 13),
+        "tbmd_bounds_report": (i32, [pi64, pi32, pi64, pi64]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

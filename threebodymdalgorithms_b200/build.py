@@ -1,7 +1,12 @@
 """Build the native parts in-tree: libtbmd.so (CUDA kernels + C ABI, sm_100a) and the drop-in
 executable tbmd_main (C++ host, the reference's CLI and CSV contract, linked against libtbmd.so).
 
-    python -m threebodymdalgorithms_b200.build [--force]
+    python -m threebodymdalgorithms_b200.build [--force] [--bounds-check]
+
+--bounds-check also builds libtbmd_checked.so, the same library compiled with -DTBMD_BOUNDS_CHECK:
+every checked kernel index outside its array is recorded on the device (and replaced by 0, so the
+kernel runs on without faulting) and read back with tbmd_bounds_report.  Point TBMD_LIBRARY at it to
+run a program or the test suite on the checked build.
 """
 from __future__ import annotations
 
@@ -14,6 +19,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 INCLUDE = PKG.parent / "include"
 LIB = PKG / "libtbmd.so"
+LIB_CHECKED = PKG / "libtbmd_checked.so"
 MAIN = PKG / "tbmd_main"
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -39,13 +45,15 @@ def _run(cmd):
     return r
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
+def build(force: bool = False, verbose: bool = False, bounds_check: bool = False) -> Path:
     deps = [CSRC / s for s in CU_SOURCES] + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
-    if force or _stale(LIB, deps):
-        cmd = [NVCC] + NVFLAGS + ["-shared", "-o", str(LIB)] + [str(CSRC / s) for s in CU_SOURCES]
-        if verbose:
-            print(" ".join(cmd))
-        _run(cmd)
+    targets = [(LIB, [])] + ([(LIB_CHECKED, ["-DTBMD_BOUNDS_CHECK"])] if bounds_check else [])
+    for target, extra in targets:
+        if force or _stale(target, deps):
+            cmd = [NVCC] + NVFLAGS + extra + ["-shared", "-o", str(target)] + [str(CSRC / s) for s in CU_SOURCES]
+            if verbose:
+                print(" ".join(cmd))
+            _run(cmd)
     main_deps = [CSRC / "tbmd_main.cpp", INCLUDE / "tbmd.h", LIB]
     if (CSRC / "tbmd_main.cpp").exists() and (force or _stale(MAIN, main_deps)):
         cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-pthread", "-I", str(INCLUDE), str(CSRC / "tbmd_main.cpp"), "-o",
@@ -57,5 +65,5 @@ def build(force: bool = False, verbose: bool = False) -> Path:
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True)
+    build(force="--force" in sys.argv, verbose=True, bounds_check="--bounds-check" in sys.argv)
     print(LIB)

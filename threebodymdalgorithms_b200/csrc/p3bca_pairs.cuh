@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(256, P3PairMinBlocks<S>::value)
         bool nowrap = true;
         for (int e = lane; e < Ms; e += 32) {
             const int pos_in_list = e < mI ? offI + e : offJ + (e - mI);
-            const int32_t t = cb.nbr[(int64_t)s * cap + pos_in_list];
+            const int32_t t = (int32_t)TBMD_IX(cb.nbr[(int64_t)s * cap + pos_in_list], n, BS_LIST);
             GIDX[e] = t;
             const double ddx = cb.xs[t] - xi, ddy = cb.ys[t] - yi, ddz = cb.zs[t] - zi;
             nowrap = nowrap && fabs(ddx) <= cwrap && fabs(ddy) <= cwrap && fabs(ddz) <= cwrap;
@@ -353,13 +353,13 @@ __global__ void __launch_bounds__(256, P3PairMinBlocks<S>::value)
                         // the row ends inside this lane's range: close its segment, go to the next
                         // row with pairs
                         if (seg >= 0)
-                            SEGR[seg] = racc;
+                            SEGR[TBMD_IX(seg, a1, BS_PAIR_SEG)] = racc;
                         else
-                            SEGL[-1 - seg] = racc;
+                            SEGL[TBMD_IX(-1 - seg, 32, BS_PAIR_SEG)] = racc;
                         racc = slot4_zero<S>();
                         do {
                             ++a;
-                            mask = RMASK[a];
+                            mask = RMASK[TBMD_IX(a, a1, BS_PAIR_ROW)];
                         } while (mask == 0ull && a + 1 < a1);
                         seg = a;
                         od = EH[a];
@@ -373,14 +373,14 @@ __global__ void __launch_bounds__(256, P3PairMinBlocks<S>::value)
                     }
                     const int j = __ffsll((long long)mask) - 1;
                     mask &= mask - 1ull;
-                    const Slot4<S> pd = EH[c0 + j];
+                    const Slot4<S> pd = EH[TBMD_IX(c0 + j, Ms, BS_SLOT)];
                     const V3<S> v = {pd.x, pd.y, pd.z};
                     V3<S> vl = vzero<S>();
                     if (L::lo) {
                         const Slot4<S> pl = EL[c0 + j];
                         vl = {pl.x, pl.y, pl.z};
                     }
-                    const ColMeta cm = COL[j];
+                    const ColMeta cm = COL[TBMD_IX(j, C, BS_PAIR_COL)];
                     const V3<S> w = third_edge(u, ul, v, vl);
                     const ATCoef<S> cf = at_coef<ENERGY>(aa, pd.w, dot3(w, w), dot3(u, v), dot3(u, w), dot3(v, w),
                                                          nu, nu3, nu15, true, en);
@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(256, P3PairMinBlocks<S>::value)
                     racc.w = racc.w + cf.alpha;
                     const int place = cm.base + __popc(cm.lo & (unsigned)below_a) +
                                       __popc(cm.hi & (unsigned)(below_a >> 32));
-                    PART[place] = Slot4<S>{gw.x, gw.y, gw.z, cf.beta};
+                    PART[TBMD_IX(place, P, BS_PAIR_PLACE)] = Slot4<S>{gw.x, gw.y, gw.z, cf.beta};
                 }
                 if (seg >= 0)
                     SEGR[seg] = racc;
@@ -468,7 +468,8 @@ __global__ void __launch_bounds__(256, P3PairMinBlocks<S>::value)
         unsigned int wn = 0;
         if (lane == 0) wn = atomicAdd(cb.work_counter + 1, 1u);
         const unsigned long long it = cb.long_items[wk];
-        const int s = (int)(it >> 32), I = (int)((it >> 16) & 0xffffu), J = (int)(it & 0xffffu);
+        const int s = (int)TBMD_IX((int64_t)(it >> 32), n, BS_LONG_ITEM), I = (int)((it >> 16) & 0xffffu),
+                  J = (int)(it & 0xffffu);
         const int M = min(cb.nbr_count[s], cap);
         const int mI = min(P3_CHUNK, M - I * P3_CHUNK);
         const int mJ = J != I ? min(P3_CHUNK, M - J * P3_CHUNK) : 0;

@@ -1264,6 +1264,23 @@ tbmd_status tbmd_sync(tbmd_ctx *ctx)
 
 const char *tbmd_tuning(const tbmd_ctx *ctx) { return ctx ? ctx->tuning.c_str() : "{}"; }
 
+int32_t tbmd_bounds_report(int64_t *violations, int32_t *site, int64_t *index, int64_t *size)
+{
+    BoundsRecord k{}, gen{};
+    const bool ok = cudaDeviceSynchronize() == cudaSuccess && bounds_read_kernels(&k) == cudaSuccess &&
+                    bounds_read_gen(&gen) == cudaSuccess;
+    const BoundsRecord &first = k.count ? k : gen;
+    if (violations) *violations = ok ? (int64_t)k.count + (int64_t)gen.count : -1;
+    if (site) *site = first.site;
+    if (index) *index = first.index;
+    if (size) *size = first.size;
+#ifdef TBMD_BOUNDS_CHECK
+    return 1;
+#else
+    return 0;
+#endif
+}
+
 tbmd_status tbmd_set_profiling(tbmd_ctx *ctx, int32_t on)
 {
     if (!ctx) return TBMD_INVALID_ARG;

@@ -236,10 +236,11 @@ __global__ void __launch_bounds__(GEN_BLOCK) k_polar_place(uint64_t x0, uint64_t
     double *dst = axis == 0 ? x : (axis == 1 ? y : z);
     const double *cen = axis == 0 ? cxs : (axis == 1 ? cys : czs);
     const double v0 = __dadd_rn(__dmul_rn(__dmul_rn(a.y, mult), stddev), mean);
-    dst[q0] = __dadd_rn(cen[q0 / per], v0);
+    const int64_t ncen = (m + per - 1) / per;
+    dst[TBMD_IX(q0, m, BS_GEN)] = __dadd_rn(cen[TBMD_IX(q0 / per, ncen, BS_GEN)], v0);
     if (q0 + 1 < m) {
         const double v1 = __dadd_rn(__dmul_rn(__dmul_rn(a.x, mult), stddev), mean);
-        dst[q0 + 1] = __dadd_rn(cen[(q0 + 1) / per], v1);
+        dst[q0 + 1] = __dadd_rn(cen[TBMD_IX((q0 + 1) / per, ncen, BS_GEN)], v1);
     }
 }
 
@@ -355,6 +356,22 @@ cudaError_t launch_polar_pass(uint64_t x0, uint64_t t0, int64_t T, unsigned long
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     return cudaMemcpyAsync(accepted_end, start + nb, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+}
+
+
+// The bounds-check record of this translation unit (see TBMD_IX), read and cleared; zero when the
+// library was built without the checks.
+cudaError_t bounds_read_gen(BoundsRecord *out)
+{
+#ifdef TBMD_BOUNDS_CHECK
+    cudaError_t e = cudaMemcpyFromSymbol(out, g_bounds_record, sizeof(BoundsRecord));
+    if (e != cudaSuccess) return e;
+    const BoundsRecord zero{};
+    return cudaMemcpyToSymbol(g_bounds_record, &zero, sizeof(BoundsRecord));
+#else
+    *out = BoundsRecord{};
+    return cudaSuccess;
+#endif
 }
 
 }  // namespace tbmd

@@ -221,6 +221,57 @@ __device__ __forceinline__ Dual<float> dot_uv<Dual<float>>(V3<Dual<float>> uh, V
 }
 
 // ---------------------------------------------------------------------------------------------
+// Debug-build index checks.  Compiled with -DTBMD_BOUNDS_CHECK (libtbmd_checked.so),
+// TBMD_IX(i, size, site) passes an index i inside [0, size) through and otherwise records it (the
+// first violation's site, index and size, and a count) in a device-side record of its translation
+// unit and yields 0, so the access stays inside the array and the kernel runs on: nothing traps and
+// no wait is involved.  The host reads and clears the records with tbmd_bounds_report.  In the
+// normal build TBMD_IX(i, size, site) is i.  Sites are numbered in BoundsSite.
+struct BoundsRecord {
+    unsigned int count;
+    int site;
+    long long index, size;
+};
+enum BoundsSite : int {
+    BS_CELL_OF = 1,       // cell of a particle (assign, predictor-assign)
+    BS_CELL_SLOT,         // sorted slot of a particle (scatter)
+    BS_SORTED,            // sorted index -> input index (gather, unsort)
+    BS_NBR_CELL,          // neighbour-cell table entry
+    BS_STAGE,             // neighbour kernel staging place
+    BS_CANDIDATE,         // neighbour kernel candidate particle
+    BS_LIST,              // half-list entry (sorted index)
+    BS_LONG_ITEM,         // chunk-pair item
+    BS_SLOT,              // staged slot of a triplet item
+    BS_PAIR_ROW,          // pair kernel row
+    BS_PAIR_COL,          // pair kernel column
+    BS_PAIR_PLACE,        // pair kernel staging place
+    BS_PAIR_SEG,          // pair kernel segment record
+    BS_SWEEP,             // AUTA / NATA particle index
+    BS_PARTIAL,           // NATA partial-sum slot
+    BS_SYSTEM,            // system of a batched item
+    BS_GEN,               // generator word / particle
+};
+#ifdef TBMD_BOUNDS_CHECK
+static __device__ BoundsRecord g_bounds_record;
+__device__ __forceinline__ long long tbmd_ix(long long i, long long size, int site)
+{
+    if (i >= 0 && i < size) return i;
+    if (atomicAdd(&g_bounds_record.count, 1u) == 0u) {
+        g_bounds_record.site = site;
+        g_bounds_record.index = i;
+        g_bounds_record.size = size;
+    }
+    return 0;
+}
+#define TBMD_IX(i, size, site) tbmd_ix((long long)(i), (long long)(size), (site))
+#else
+#define TBMD_IX(i, size, site) (i)
+#endif
+// Host side: this translation unit's record (a zero record in the normal build), cleared after reading.
+cudaError_t bounds_read_kernels(BoundsRecord *out);
+cudaError_t bounds_read_gen(BoundsRecord *out);
+
+// ---------------------------------------------------------------------------------------------
 // Kernel argument blocks.
 
 // Positions (FP64 SoA) and, for the adjoint, the direction vector (cotangent on the forces).

@@ -175,7 +175,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
         unsigned int wn = 0;
         if (lane == 0) wn = atomicAdd(work.counter, 1u);
         // system, then (block, i) inside it
-        const int sys = work.nsys > 1 ? find_block(work.sys_items, work.nsys, (int64_t)w) : 0;
+        const int sys = (int)TBMD_IX(work.nsys > 1 ? find_block(work.sys_items, work.nsys, (int64_t)w) : 0, work.nsys,
+                                     BS_SYSTEM);
         const int64_t wl = (int64_t)w - work.sys_items[sys];
         const int64_t off = work.sys_off[sys], hi = work.sys_off[sys + 1];
         const int64_t *prefix = work.prefix + work.sys_prefix[sys];
@@ -188,6 +189,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out
             kbeg += (r % nseg) * work.kseg;
             kend = min(hi, kbeg + work.kseg);
         }
+        i = TBMD_IX(i, n, BS_SWEEP);
         const double xi = pos.x[i], yi = pos.y[i], zi = pos.z[i];
         double dxi = 0.0, dyi = 0.0, dzi = 0.0;
         if (Traits<S>::dual) {
@@ -308,7 +310,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_nata(int64_t n, Pos pos, double 
         unsigned int wn = 0;
         if (lane == 0) wn = atomicAdd(work.counter, 1u);
         const int b = (int)((int64_t)w / n);
-        const int64_t i = (int64_t)w - (int64_t)b * n;
+        const int64_t i = TBMD_IX((int64_t)w - (int64_t)b * n, n, BS_SWEEP);
         const double xi = pos.x[i], yi = pos.y[i], zi = pos.z[i];
         V3<S> u[R], ul[R];
         S aa[R];
@@ -378,7 +380,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_nata(int64_t n, Pos pos, double 
         }
         g = warp_sum3(g);
         if (lane == 0) {
-            double *dst = partial + ((int64_t)i * nb + b) * 3;
+            double *dst = partial + TBMD_IX(((int64_t)i * nb + b) * 3, n * nb * 3, BS_PARTIAL);
             dst[0] = -acc_value(g.x);
             dst[1] = -acc_value(g.y);
             dst[2] = -acc_value(g.z);
@@ -558,6 +560,7 @@ __global__ void k_cell_assign(int64_t n, const double *__restrict__ x, const dou
     int cy = cell_coord_w(y[i], G.lo[1], G.w[1], G.dims[1], out);
     int cz = cell_coord_w(z[i], G.lo[2], G.w[2], G.dims[2], out);
     int c = (int)(set.nsys > 1 ? set.cell_off[sys] : 0) + (cz * G.dims[1] + cy) * G.dims[0] + cx;
+    c = (int)TBMD_IX(c, g.ncells, BS_CELL_OF);
     cell_of[i] = c;
     atomicAdd(cell_count + c, 1);
     if (out) cell_out[c] = 1;
@@ -596,7 +599,7 @@ __global__ void k_cell_scatter(int64_t n, const int32_t *__restrict__ cell_of, c
     if (i >= n) return;
     int c = cell_of[i];
     int slot = atomicAdd(fill + c, 1);
-    sorted[start[c] + slot] = (int32_t)i;
+    sorted[TBMD_IX(start[c] + slot, n, BS_CELL_SLOT)] = (int32_t)i;
 }
 
 // Positions (and the adjoint direction) in sorted order, plus the FP32 hi/lo copy relative to the
@@ -607,7 +610,7 @@ __global__ void k_gather(int64_t n, const int32_t *__restrict__ sorted, Pos pos,
 {
     int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
-    int32_t i = sorted[s];
+    int32_t i = (int32_t)TBMD_IX(sorted[s], n, BS_SORTED);
     const double x = pos.x[i], y = pos.y[i], z = pos.z[i];
     xs[s] = x;
     ys[s] = y;
@@ -669,7 +672,7 @@ __global__ void k_predict_assign(int64_t n, double *x, double *y, double *z, con
     const int cx = cell_coord_w(px, g.lo[0], g.w[0], g.dims[0], out);
     const int cy = cell_coord_w(py, g.lo[1], g.w[1], g.dims[1], out);
     const int cz = cell_coord_w(pz, g.lo[2], g.w[2], g.dims[2], out);
-    const int c = (cz * g.dims[1] + cy) * g.dims[0] + cx;
+    const int c = (int)TBMD_IX((cz * g.dims[1] + cy) * g.dims[0] + cx, g.ncells, BS_CELL_OF);
     cell_of[i] = c;
     atomicAdd(cell_count + c, 1);
     if (out) cell_out[c] = 1;
@@ -684,7 +687,7 @@ __global__ void k_scatter_gather(int64_t n, const int32_t *__restrict__ cell_of,
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int c = cell_of[i];
-    const int slot = start[c] + atomicAdd(fill + c, 1);
+    const int slot = (int)TBMD_IX(start[c] + atomicAdd(fill + c, 1), n, BS_CELL_SLOT);
     sorted[slot] = (int32_t)i;
     const double px = x[i], py = y[i], pz = z[i];
     xs[slot] = px;
@@ -785,7 +788,7 @@ cudaError_t launch_unsort_update(int64_t n, const CellBufs &cb, double *const st
 constexpr int NB_THREADS = 128;
 constexpr size_t NB_STAGE_BYTES = 2 * sizeof(float4) + sizeof(int32_t);  // per staged candidate
 
-__global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(const __grid_constant__ Grid g, GridSet set,
+__global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(int64_t n, const __grid_constant__ Grid g, GridSet set,
                                                           const int32_t *__restrict__ nbr_cells,
                                                           const float4 *__restrict__ qhi,
                                                           const float4 *__restrict__ qlo,
@@ -815,7 +818,8 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(const __grid_const
         const float Lx = (float)G.L[0], Ly = (float)G.L[1], Lz = (float)G.L[2];
         const float sq_lo = (float)G.sqcut - G.band, sq_hi = (float)G.sqcut + G.band;
         if (warp == 0) {
-            const int nc = lane < 27 ? nbr_cells[c * 27 + lane] : -1;
+            int nc = lane < 27 ? nbr_cells[c * 27 + lane] : -1;
+            if (nc >= 0) nc = (int)TBMD_IX(nc, g.ncells, BS_NBR_CELL);
             const int cs = nc >= 0 ? cell_start[nc] : 0;
             const int len = nc >= 0 ? cell_start[nc + 1] - cs : 0;
             // raw test: an interior cell (at least 4 cells per axis, not on the boundary, so no
@@ -859,7 +863,8 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(const __grid_const
             for (int q = threadIdx.x; q < T + 32; q += NB_THREADS) {
                 if (q < T) {
                     const int k = entry_of(q);
-                    const int t = cstart[k] + (q - cpre[k]);
+                    const int t = (int)TBMD_IX(cstart[k] + (q - cpre[k]), n, BS_CANDIDATE);
+                    (void)TBMD_IX(q, max_stage, BS_STAGE);
                     shi[q] = qhi[t];
                     slo[q] = qlo[t];
                     st[q] = t;
@@ -921,7 +926,7 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(const __grid_const
                     int t = 0;
                     if (q < T) {
                         const int k = entry_of(q);
-                        t = cstart[k] + (q - cpre[k]);
+                        t = (int)TBMD_IX(cstart[k] + (q - cpre[k]), n, BS_CANDIDATE);
                         const float4 h = qhi[t];
                         float d2;
                         if (raw) {
@@ -1015,12 +1020,11 @@ void neighbor_cell_table(const Grid &g, int64_t cell0, int32_t *out)
 cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, const int32_t *nbr_cells, int max_stage,
                              CellBufs &cb, cudaStream_t st)
 {
-    (void)n;
     const size_t smem = (size_t)max_stage * NB_STAGE_BYTES;
     int64_t blocks = g.ncells < 65535 * 16 ? g.ncells : 65535 * 16;
     cudaError_t e = cudaMemsetAsync(cb.long_count, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return e;
-    k_neighbors<<<(unsigned)blocks, NB_THREADS, smem, st>>>(g, set, nbr_cells, cb.qhi, cb.qlo, cb.xs, cb.ys, cb.zs,
+    k_neighbors<<<(unsigned)blocks, NB_THREADS, smem, st>>>(n, g, set, nbr_cells, cb.qhi, cb.qlo, cb.xs, cb.ys, cb.zs,
                                                             cb.cell_start, cb.cell_out, cb.nbr, cb.nbr_count,
                                                             cb.max_count, cb.cap,
                                                             max_stage, cb.long_items, (unsigned int)cb.long_cap,
@@ -1351,7 +1355,7 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
         bool nowrap = true;
         for (int e = lane; e < Ms; e += 32) {
             const int pos_in_list = e < mI ? offI + e : offJ + (e - mI);
-            const int32_t t = cb.nbr[(int64_t)s * cap + pos_in_list];
+            const int32_t t = (int32_t)TBMD_IX(cb.nbr[(int64_t)s * cap + pos_in_list], n, BS_LIST);
             W.idx[e] = t;
             const double x = cb.xs[t], y = cb.ys[t], z = cb.zs[t];
             const double ddx = x - xi, ddy = y - yi, ddz = z - zi;
@@ -1514,7 +1518,8 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
         unsigned int wn = 0;
         if (lane == 0) wn = atomicAdd(cb.work_counter + 1, 1u);
         const unsigned long long it = cb.long_items[w];
-        const int s = (int)(it >> 32), I = (int)((it >> 16) & 0xffffu), J = (int)(it & 0xffffu);
+        const int s = (int)TBMD_IX((int64_t)(it >> 32), n, BS_LONG_ITEM), I = (int)((it >> 16) & 0xffffu),
+                  J = (int)(it & 0xffffu);
         const int M = min(cb.nbr_count[s], cap);
         const int mI = min(P3_CHUNK, M - I * P3_CHUNK);
         const int mJ = J != I ? min(P3_CHUNK, M - J * P3_CHUNK) : 0;
@@ -1678,7 +1683,7 @@ __global__ void k_unsort(int64_t n, const int32_t *__restrict__ sorted, const do
 {
     int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
-    int32_t i = sorted[s];
+    int32_t i = (int32_t)TBMD_IX(sorted[s], n, BS_SORTED);
     o0[i] = f0[s];
     o1[i] = f1[s];
     o2[i] = f2[s];
@@ -1886,6 +1891,22 @@ double key_to_double(unsigned long long key)
     double d;
     std::memcpy(&d, &b, sizeof d);
     return d;
+}
+
+
+// The bounds-check record of this translation unit (see TBMD_IX), read and cleared; zero when the
+// library was built without the checks.
+cudaError_t bounds_read_kernels(BoundsRecord *out)
+{
+#ifdef TBMD_BOUNDS_CHECK
+    cudaError_t e = cudaMemcpyFromSymbol(out, g_bounds_record, sizeof(BoundsRecord));
+    if (e != cudaSuccess) return e;
+    const BoundsRecord zero{};
+    return cudaMemcpyToSymbol(g_bounds_record, &zero, sizeof(BoundsRecord));
+#else
+    *out = BoundsRecord{};
+    return cudaSuccess;
+#endif
 }
 
 }  // namespace tbmd
