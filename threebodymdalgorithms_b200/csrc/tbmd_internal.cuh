@@ -242,10 +242,6 @@ enum BoundsSite : int {
     BS_LIST,              // half-list entry (sorted index)
     BS_LONG_ITEM,         // chunk-pair item
     BS_SLOT,              // staged slot of a triplet item
-    BS_PAIR_ROW,          // pair kernel row
-    BS_PAIR_COL,          // pair kernel column
-    BS_PAIR_PLACE,        // pair kernel staging place
-    BS_PAIR_SEG,          // pair kernel segment record
     BS_SWEEP,             // AUTA / NATA particle index
     BS_PARTIAL,           // NATA partial-sum slot
     BS_SYSTEM,            // system of a batched item
@@ -308,8 +304,6 @@ struct Grid {
     float raw_lo;   // FP32 third-edge test without wrapping, hi + lo edges: d2 <= raw_lo is inside,
     float raw_hi;   // d2 > raw_hi outside, the exact test in between
     int raw_ok;     // every box length >= 4 cutoffs: raw distance = periodic formula for non-wrapping pairs
-    float hi_lo;    // FP32 test on the hi parts of edges that do not wrap (k_p3pair's adjacency):
-    float hi_hi;    //   d2 <= hi_lo inside, d2 > hi_hi outside, the exact test in between
 };
 
 // Several independent systems packed back to back: system s owns particles (and sorted slots)

@@ -1529,8 +1529,6 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
     flush(cur_sys);
 }
 
-#include "p3bca_pairs.cuh"
-
 void fill_grid_test_params(Grid &g);
 
 // Half-width of the uncertainty band around cutoff^2 of the guarded third-edge test, for unit
@@ -1572,15 +1570,6 @@ static int raw_test_ok(const Grid &g)
 // band of the wrapped form, whose L - |d| carries errors of order 2^-24 L.
 static double raw_band(const Grid &g) { return 36.0 / 16777216.0 * g.sqcut; }  // 2^-24
 
-// Half-width of the band of the FP32 adjacency test of k_p3pair on the hi parts alone of edges that
-// do not wrap (each component within the cutoff c of s).  hi = fl32(e) differs from the FP64 edge e
-// by at most 2^-24 |e_i| per component, so a component of w = hi_q - hi_p, rounded once more, is
-// within 2^-24 (|e_p,i| + |e_q,i| + |w_i|) <= 4 * 2^-24 c of the reference's x_q - x_p (|w| <= 2 c).
-// The squared length then differs from the reference's by at most 8 sqrt(3) 2^-24 c |w| (about
-// 13.9 * 2^-24 c^2 near the cutoff), plus 3 * 2^-24 c^2 from its own three roundings and 2^-24 c^2
-// from rounding the thresholds: 18 * 2^-24 c^2.  Four times that is used.
-static double hi_band(const Grid &g) { return 72.0 / 16777216.0 * g.sqcut; }
-
 void fill_grid_test_params(Grid &g)
 {
     g.band = (float)guard_band(g, 1.0 / 8388608.0);      // 2^-23
@@ -1588,28 +1577,6 @@ void fill_grid_test_params(Grid &g)
     g.raw_lo = (float)(g.sqcut - raw_band(g));
     g.raw_hi = (float)(g.sqcut + raw_band(g));
     g.raw_ok = raw_test_ok(g);
-    g.hi_lo = (float)(g.sqcut - hi_band(g));
-    g.hi_hi = (float)(g.sqcut + hi_band(g));
-}
-
-// The forces (FP32 and FP64 geometry, with or without the energy) run the pair-compacted k_p3pair;
-// the adjoint (dual types) runs k_p3bca.
-template <class S, bool ENERGY>
-static auto p3_kernel()
-{
-    if constexpr (Traits<S>::dual)
-        return k_p3bca<S, ENERGY>;
-    else
-        return k_p3pair<S, ENERGY>;
-}
-
-template <class S>
-static size_t p3_warp_bytes()
-{
-    if constexpr (Traits<S>::dual)
-        return (size_t)2 * P3_CHUNK * SlotLayout<S>::bytes_per_slot;
-    else
-        return PairLayout<S>::bytes;
 }
 
 template <class S>
@@ -1620,14 +1587,14 @@ static cudaError_t plan_p3bca_t(bool energy, int cap, int warps, P3Plan *plan)
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     (void)cap;
-    const size_t per_warp = p3_warp_bytes<S>();
+    const size_t per_warp = (size_t)2 * P3_CHUNK * SlotLayout<S>::bytes_per_slot;
     const size_t smem_cap = 220 * 1024;
     if (warps < 1) warps = 1;
     if (warps > 8) warps = 8;
     while (warps > 1 && per_warp * warps > smem_cap) --warps;
     if (per_warp * warps > smem_cap) return cudaErrorInvalidValue;
     const size_t smem = per_warp * warps;
-    auto kern = energy ? p3_kernel<S, true>() : p3_kernel<S, false>();
+    auto kern = energy ? k_p3bca<S, true> : k_p3bca<S, false>;
     if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
         return e;
     int per_sm = 0;
@@ -1659,7 +1626,7 @@ static cudaError_t launch_p3bca_t(bool energy, int64_t n, const Grid &g, const G
 {
     cudaError_t e;
     if ((e = cudaMemsetAsync(cb.work_counter, 0, 2 * sizeof(unsigned int), st)) != cudaSuccess) return e;
-    auto kern = energy ? p3_kernel<S, true>() : p3_kernel<S, false>();
+    auto kern = energy ? k_p3bca<S, true> : k_p3bca<S, false>;
     kern<<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, set, cb, nu, eo, co);
     return cudaGetLastError();
 }
