@@ -566,30 +566,41 @@ __global__ void k_cell_assign(int64_t n, const double *__restrict__ x, const dou
     if (out) cell_out[c] = 1;
 }
 
-// Exclusive scan of cell counts (single block of 1024 threads, each owning a contiguous chunk).
+// Exclusive scan of cell counts (single block of 1024 threads, each owning a contiguous chunk; the
+// chunk totals are scanned with warp shuffles, then across the 32 warps).
 __global__ void __launch_bounds__(1024) k_cell_scan(int64_t ncells, const int32_t *__restrict__ count,
                                                     int32_t *__restrict__ start)
 {
-    __shared__ int32_t part[1024];
-    const int t = threadIdx.x;
+    __shared__ int32_t wsum[32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int64_t chunk = (ncells + 1023) / 1024;
     const int64_t b = t * chunk, e = (b + chunk < ncells) ? b + chunk : ncells;
     int32_t s = 0;
     for (int64_t c = b; c < e; ++c) s += count[c];
-    part[t] = s;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        int32_t v = t >= off ? part[t - off] : 0;
-        __syncthreads();
-        part[t] += v;
-        __syncthreads();
+    int32_t inc = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
     }
-    int32_t run = part[t] - s;
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        int32_t w = wsum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t v = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += v;
+        }
+        wsum[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    int32_t run = (warp > 0 ? wsum[warp - 1] : 0) + inc - s;
     for (int64_t c = b; c < e; ++c) {
         start[c] = run;
         run += count[c];
     }
-    if (t == 1023) start[ncells] = part[1023];
+    if (t == 1023) start[ncells] = wsum[31];
 }
 
 __global__ void k_cell_scatter(int64_t n, const int32_t *__restrict__ cell_of, const int32_t *__restrict__ start,
