@@ -13,6 +13,7 @@
 // the same for every P.  -layoutonly prints that layout as JSON and exits without touching the GPU.
 // GPU options: -prec fp64|mixed, -nu V (AT strength, default 1.0 as main.cpp:41), -device N,
 // -nograph, -tune CACHE.JSONL (autotuner), -dumpfull FILE (state at %.17g after the run),
+// -checkpoint FILE (the state after the run as an input CSV at 17 digits: -csv FILE resumes exactly),
 // -parseonly (print the parsed arguments as JSON and exit without touching the GPU).
 // -op FILE writes the profile document of the reference's PROFILE_3BMDA build (main.cpp:127-451):
 // "times" per timer (time unit, avg/total over ranks, per-rank lists), "hitrate" (triplets inside
@@ -59,7 +60,7 @@ struct Args {
     int device = 0;
     bool graph = true;
     bool parseOnly = false;
-    std::string tuneCache, dumpFull;
+    std::string tuneCache, dumpFull, checkpoint;
 };
 
 // The first 15 lines are the reference's help text byte for byte (cli.hpp:27-45), including its
@@ -87,7 +88,9 @@ void printHelp()
               << "GPU options:\n"
               << "\t-prec\t\tfp64 | mixed\n\t-nu\t\tAT strength (1.0)\n\t-device\t\tCUDA device\n"
               << "\t-nograph\t\tno CUDA graph\n\t-tune\t\tautotuner cache file\n"
-              << "\t-dumpfull\t\twrite the final state with 17 digits\n\t-opsteps\t\tper-step timings (json lines)\n"
+              << "\t-dumpfull\t\twrite the final state with 17 digits\n"
+              << "\t-checkpoint\t\twrite the final state as an input CSV with 17 digits (restart with -csv)\n"
+              << "\t-opsteps\t\tper-step timings (json lines)\n"
               << "\t-parseonly\t\tprint parsed args\n"
               << "\t-np\t\tMPI ranks of the reference run to reproduce (layout and checks; default 1)\n"
               << "\t-layoutonly\t\tprint the rank layout as JSON and exit\n"
@@ -165,6 +168,8 @@ Args parse(const std::vector<std::string> &args)
                 a.tuneCache = value();
             } else if (isFlag(f, "dumpfull", "-dumpfull")) {
                 a.dumpFull = value();
+            } else if (isFlag(f, "checkpoint", "-checkpoint")) {
+                a.checkpoint = value();
             } else if (isFlag(f, "opsteps", "-opsteps")) {
                 a.outputSteps = value();
             } else if (isFlag(f, "parseonly", "-parseonly")) {
@@ -338,6 +343,25 @@ void writeStepCSV(const std::string &path, const State &s, const std::vector<siz
     std::ofstream out(path);
     out << "ID, pX, pY, pZ, vX, vY, vZ, aX, aY, aZ, m, fX, fY, fZ\n";
     for (const std::string &part : parts) out << part;
+}
+
+// The state as an input file of the reference's format (utility.cpp:14-24: header, then ID and the
+// ten columns pX..pZ, vX..vZ, aX..aZ, m that the reader takes), with the forces appended as three more
+// columns, which the reader ignores.  Every value at 17 significant digits, so reading it back with
+// -csv restores the state exactly: an exact checkpoint, where the per-step output keeps the reference's
+// 6 digits.  A restarted P3BCA run takes its periodic domain from these positions, as the reference's
+// Init does for any input file (RegularGridDecomposition.cpp:135-166).
+bool writeCheckpoint(const std::string &path, const State &s)
+{
+    FILE *f = std::fopen(path.c_str(), "w");
+    if (!f) return false;
+    std::fprintf(f, "ID, pX, pY, pZ, vX, vY, vZ, aX, aY, aZ, m, fX, fY, fZ\n");
+    for (size_t i = 0; i < s.id.size(); ++i) {
+        std::fprintf(f, "%d", s.id[i]);
+        for (int k = 0; k < 13; ++k) std::fprintf(f, ", %.17g", s.v[k][i]);
+        std::fprintf(f, "\n");
+    }
+    return std::fclose(f) == 0;
 }
 
 void writeFull(const std::string &path, const State &s, const std::vector<uint64_t> &counts)
@@ -543,9 +567,10 @@ int main(int argc, char **argv)
             prof << "{\"allTimes\": [" << stepNs[i] << "], \"max\": " << stepNs[i] << ", \"triplets\": " << counts[i]
                  << "}\n";
     }
-    if (!a.dumpFull.empty() && n > 0) {
+    if ((!a.dumpFull.empty() || !a.checkpoint.empty()) && n > 0) {
         if (!fetch(ctx, n, s)) die("get_particles");
-        writeFull(a.dumpFull, s, counts);
+        if (!a.dumpFull.empty()) writeFull(a.dumpFull, s, counts);
+        if (!a.checkpoint.empty() && !writeCheckpoint(a.checkpoint, s)) die("checkpoint");
     }
     tbmd_destroy(ctx);
     return 0;
