@@ -341,6 +341,16 @@ def run_ours(args, world, rank, local):
                                           *[dptr(outs[k]) for k in OUT]))
             return int(cnt[0])
 
+        KSTEPS = 10
+        cnt_k = np.zeros(KSTEPS, dtype=np.uint64)
+
+        def e2e_ksteps():
+            # the same call with K steps: the copies are paid once per K steps
+            ctx._check(lib.tbmd_step_host(ctx.handle, n, ids.ctypes.data_as(ip), *[dptr(pinned[k]) for k in IN],
+                                          KSTEPS, cnt_k.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                          out_ids.ctypes.data_as(ip), *[dptr(outs[k]) for k in OUT]))
+            return int(cnt_k.sum())
+
         def e2e_separate():
             ctx._check(lib.tbmd_set_particles(ctx.handle, n, ids.ctypes.data_as(ip), *[dptr(pinned[k]) for k in IN]))
             c = ctx.step(1)
@@ -367,10 +377,18 @@ def run_ours(args, world, rank, local):
 
         tot, e2e_all = e2e_time(e2e_fused)
         tot_sep, _ = e2e_time(e2e_separate)
+        ksteps = max(1, min(args.steps, 10))
+        saved_steps, args.steps = args.steps, ksteps
+        tot_k, trip_k = e2e_time(e2e_ksteps)
+        args.steps = saved_steps
         e2e = {"value": e2e_all / (tot * 1e-3), "unit": "triplets/s", "ms_per_step": tot / args.steps,
                "h2d_bytes_per_step": 10 * 8 * n + 4 * n, "d2h_bytes_per_step": 13 * 8 * n + 4 * n,
                "path": "tbmd_step_host (state in, step, state out in one C-ABI call), pinned host SoA blocks",
-               "separate_calls_ms_per_step": tot_sep / args.steps}
+               "separate_calls_ms_per_step": tot_sep / args.steps,
+               "k_steps": {"k": KSTEPS, "calls": ksteps, "ms_per_step": tot_k / (ksteps * KSTEPS),
+                           "value": trip_k / (tot_k * 1e-3), "unit": "triplets/s",
+                           "h2d_bytes_per_call": 10 * 8 * n + 4 * n, "d2h_bytes_per_call": 13 * 8 * n + 4 * n,
+                           "path": "tbmd_step_host with K steps per call (state in, K steps, state out)"}}
         ctx.close()
 
     cpu = None
