@@ -79,11 +79,11 @@ struct ATCoef {
 };
 
 // Shared core of one triplet from the six scalars a = u.u, b = v.v, c = w.w, p = u.v, q = u.w,
-// s = v.w with w = x_k - x_j.  Callers form each as a direct dot product of accurate edge vectors
-// (never c = a + b - 2p, which cancels when j and k are close but far from i).  `valid` false
-// gives exact zeros (masked lanes, k <= j, padding) without anything inf or NaN reaching the
-// result.  nu3 = -3 nu, nu15 = 15 nu.  Returns m = -3 nu t^5 and B2 = m + 15 nu t^5 D t^2; ENERGY
-// adds the triplet energy nu t^3 (1 - 3 D t^2) to `e`.
+// s = v.w with w = x_k - x_j, passed as ab = a b, c, p and qs = q s.  Callers form each scalar as a
+// direct dot product of accurate edge vectors (never c = a + b - 2p, which cancels when j and k are
+// close but far from i).  `valid` false gives exact zeros (masked lanes, k <= j, padding) without
+// anything inf or NaN reaching the result.  nu3 = -3 nu, nu15 = 15 nu.  Returns m = -3 nu t^5 and
+// B2 = m + 15 nu t^5 D t^2; ENERGY adds the triplet energy nu t^3 (1 - 3 D t^2) to `e`.
 // One Newton step for x^(-1/2): t (1.5 - 0.5 x t^2).  Used for FP32 when the energy is also wanted:
 // the energy sum of a small system can cancel, so its terms get the refined value.
 __device__ __forceinline__ float refine_rsqrt(float x, float t) { return t * fmaf(-0.5f * x, t * t, 1.5f); }
@@ -92,33 +92,34 @@ template <class T>
 __device__ __forceinline__ Dual<T> refine_rsqrt(Dual<T>, Dual<T> t) { return t; }
 
 template <bool ENERGY, class S>
-__device__ __forceinline__ void at_core(S a, S b, S c, S p, S q, S s, S nu, S nu3, S nu15, bool valid, S &e, S &m,
-                                        S &B2)
+__device__ __forceinline__ void at_core(S ab, S c, S p, S qs, S nu, S nu3, S nu15, bool valid, S &e, S &m, S &B2)
 {
-    const S x = a * b * c;
+    const S x = ab * c;
     S t = rsqrt_(x);
     if (ENERGY) t = refine_rsqrt(x, t);
     if (!valid) t = zero_like(t);
     S t2 = t * t;
     S t5 = t2 * t2 * t;
-    S Dt2 = p * q * s * t2;
+    S Dt2 = p * qs * t2;
     m = nu3 * t5;
     B2 = t5 * fma_(nu15, Dt2, nu3);
     if (ENERGY) e = e + t2 * t * fma_(nu3, Dt2, nu);
 }
 
-// Gradient coefficients for all three particles (see the top of this file).
+// Gradient coefficients for all three particles (see the top of this file).  With P2 = p (q + s) and
+// s - q = (v - u).w = c, the three combinations are qs - ps - pq = qs - P2, qs + ps + pq = qs + P2 and
+// qs + ps - pq = qs + p c (c is the directly formed w.w, the more accurate of the two equal values).
 template <bool ENERGY, class S>
 __device__ __forceinline__ ATCoef<S> at_coef(S a, S b, S c, S p, S q, S s, S nu, S nu3, S nu15, bool valid, S &e)
 {
     S m, B2;
-    at_core<ENERGY>(a, b, c, p, q, s, nu, nu3, nu15, valid, e, m, B2);
-    S pq = p * q, ps = p * s, qs = q * s;
-    S x = qs + ps;
+    const S ab = a * b, qs = q * s;
+    at_core<ENERGY>(ab, c, p, qs, nu, nu3, nu15, valid, e, m, B2);
+    const S P2 = p * (q + s);
     ATCoef<S> r;
-    r.alpha = fma_(B2, b * c, m * (qs - (ps + pq)));
-    r.beta = fma_(B2, a * c, m * (x + pq));
-    r.gamma = fma_(m, x - pq, -(B2 * (a * b)));
+    r.alpha = fma_(B2, b * c, m * (qs - P2));
+    r.beta = fma_(B2, a * c, m * (qs + P2));
+    r.gamma = fma_(m, fma_(p, c, qs), -(B2 * ab));
     return r;
 }
 
@@ -139,8 +140,8 @@ __device__ __forceinline__ ATSelf<S> at_self(S a, S b, S c, S p, S q, S s, S nu,
                                              S &e)
 {
     S m, B2;
-    at_core<ENERGY>(a, b, c, p, q, s, nu, nu3, nu15, valid, e, m, B2);
-    S qs = q * s;
+    const S qs = q * s;
+    at_core<ENERGY>(a * b, c, p, qs, nu, nu3, nu15, valid, e, m, B2);
     ATSelf<S> r;
     r.sigma = fma_(B2, c * (a + b), (m + m) * qs);
     // beta = B2 a c + m (q s + p (q + s)),  -alpha = B2 (-b) c + m (-q s + p (q + s))
