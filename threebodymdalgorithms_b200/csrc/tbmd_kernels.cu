@@ -1166,34 +1166,6 @@ __device__ __forceinline__ void pgrad_add<float>(Grad<float> &slot, const PGrad<
     v.w = v.w + pg.beta;
     slot = v;
 }
-// partner shares of all lanes for one common partner slot, added by lane 0
-template <class S>
-__device__ __forceinline__ void pgrad_add_warp(Grad<S> &slot, const PGrad<S> &pg, int lane)
-{
-    const V3<S> g = warp_sum3s(pg.g);
-    if (lane == 0) slot_add(slot, g);
-}
-template <>
-__device__ __forceinline__ void pgrad_add_warp<float>(Grad<float> &slot, const PGrad<float> &pg, int lane)
-{
-    V3<float> g = pg.w * pg.ngamma;
-    float beta = pg.beta;
-#pragma unroll
-    for (int m = 16; m > 0; m >>= 1) {
-        g.x += __shfl_xor_sync(0xffffffffu, g.x, m);
-        g.y += __shfl_xor_sync(0xffffffffu, g.y, m);
-        g.z += __shfl_xor_sync(0xffffffffu, g.z, m);
-        beta += __shfl_xor_sync(0xffffffffu, beta, m);
-    }
-    if (lane == 0) {
-        Grad<float> v = slot;
-        v.x += g.x;
-        v.y += g.y;
-        v.z += g.z;
-        v.w += beta;
-        slot = v;
-    }
-}
 // own-slot accumulator of a lane
 template <class S>
 struct OwnAcc {
@@ -1256,7 +1228,83 @@ struct P3Warp {
     Slot4<S> *sl;  // lo edge (mixed)
     Grad<S> *gr;   // gradient accumulators
     int32_t *idx;
+    __device__ __forceinline__ Slot4<S> slot(int i) const { return sd[i]; }
+    __device__ __forceinline__ void set_slot(int i, const Slot4<S> &v) const { sd[i] = v; }
+    __device__ __forceinline__ Grad<S> grad(int i) const { return gr[i]; }
+    __device__ __forceinline__ void set_grad(int i, const Grad<S> &v) const { gr[i] = v; }
 };
+// FP64: the 32-byte slot and accumulator records are stored as two arrays of 16-byte halves, (x, y)
+// for all slots and then (z, w), so that the 16-byte accesses of a warp to consecutive slots are free
+// of bank conflicts (32-byte records read as two halves conflict two ways: 73 M of 160 M shared
+// wavefronts of a C3 launch).
+template <>
+struct P3Warp<double> {
+    static constexpr int SL = 2 * P3_CHUNK;
+    Slot4<double> *sd;  // [SL] (x, y), then [SL] (z, w), as double2
+    Slot4<double> *sl;  // unused
+    Grad<double> *gr;   // [SL] (x, y), then [SL] (z, w), as double2
+    int32_t *idx;
+    __device__ __forceinline__ Slot4<double> slot(int i) const
+    {
+        const double2 a = ((const double2 *)sd)[i], b = ((const double2 *)sd)[SL + i];
+        return Slot4<double>{a.x, a.y, b.x, b.y};
+    }
+    __device__ __forceinline__ void set_slot(int i, const Slot4<double> &v) const
+    {
+        ((double2 *)sd)[i] = make_double2(v.x, v.y);
+        ((double2 *)sd)[SL + i] = make_double2(v.z, v.w);
+    }
+    __device__ __forceinline__ Grad<double> grad(int i) const
+    {
+        const double2 a = ((const double2 *)gr)[i], b = ((const double2 *)gr)[SL + i];
+        return Grad<double>{a.x, a.y, b.x, b.y};
+    }
+    __device__ __forceinline__ void set_grad(int i, const Grad<double> &v) const
+    {
+        ((double2 *)gr)[i] = make_double2(v.x, v.y);
+        ((double2 *)gr)[SL + i] = make_double2(v.z, v.w);
+    }
+};
+// read-modify-write of slot i's accumulator with a partner share
+template <class S>
+__device__ __forceinline__ void pgrad_add_at(const P3Warp<S> &W, int i, const PGrad<S> &pg)
+{
+    Grad<S> g = W.grad(i);
+    pgrad_add(g, pg);
+    W.set_grad(i, g);
+}
+// partner shares of all lanes for one common partner slot, added by lane 0
+template <class S>
+__device__ __forceinline__ void pgrad_add_warp(const P3Warp<S> &W, int i, const PGrad<S> &pg, int lane)
+{
+    const V3<S> g = warp_sum3s(pg.g);
+    if (lane == 0) {
+        Grad<S> v = W.grad(i);
+        slot_add(v, g);
+        W.set_grad(i, v);
+    }
+}
+template <>
+__device__ __forceinline__ void pgrad_add_warp<float>(const P3Warp<float> &W, int i, const PGrad<float> &pg, int lane)
+{
+    V3<float> g = pg.w * pg.ngamma;
+    float beta = pg.beta;
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) {
+        g.x += __shfl_xor_sync(0xffffffffu, g.x, m);
+        g.y += __shfl_xor_sync(0xffffffffu, g.y, m);
+        g.z += __shfl_xor_sync(0xffffffffu, g.z, m);
+        beta += __shfl_xor_sync(0xffffffffu, beta, m);
+    }
+    if (lane == 0) {
+        Grad<float> v = W.grad(i);
+        v.x += g.x;
+        v.y += g.y;
+        v.z += g.z;
+        v.w += beta;
+        W.set_grad(i, v);
+    }
+}
 
 // Third-edge cutoff decision for slots a (own) and b (partner) with third edge w (cww = w.w).
 // sq_lo / sq_hi: the FP32 thresholds (cutoff^2 minus / plus the band of the item's test form),
@@ -1391,9 +1439,9 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
             split<S>(ddx, dual ? cb.dxs[t] - dxi : 0.0, v.x, l.x);
             split<S>(ddy, dual ? cb.dys[t] - dyi : 0.0, v.y, l.y);
             split<S>(ddz, dual ? cb.dzs[t] - dzi : 0.0, v.z, l.z);
-            W.sd[e] = Slot4<S>{v.x, v.y, v.z, dot3(v, v)};
+            W.set_slot(e, Slot4<S>{v.x, v.y, v.z, dot3(v, v)});
             if (L::nlo) W.sl[e] = Slot4<S>{l.x, l.y, l.z, szero<S>()};
-            W.gr[e] = grad_zero<S>();
+            W.set_grad(e, grad_zero<S>());
         }
         const bool rawok = G.raw_ok && __all_sync(0xffffffffu, nowrap);
         // FP32 thresholds: the narrow band of hi + lo edges that do not wrap (mixed forces), else
@@ -1420,7 +1468,7 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
                 const int mA = min(32, mI - A0);
                 const bool own = lane < mA;
                 const int a = A0 + (own ? lane : 0);
-                const Slot4<S> od = W.sd[a];
+                const Slot4<S> od = W.slot(a);
                 const V3<S> u = {od.x, od.y, od.z};
                 V3<S> ul = vzero<S>();
                 if (L::nlo) {
@@ -1433,7 +1481,7 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
 
                 // evaluate own slot a against partner slot b; returns the partner's share
                 auto pair = [&](bool act, int b) -> PGrad<S> {
-                    const Slot4<S> pd = W.sd[b];
+                    const Slot4<S> pd = W.slot(b);
                     const V3<S> v = {pd.x, pd.y, pd.z};
                     V3<S> vl = vzero<S>();
                     if (L::nlo) {
@@ -1472,7 +1520,7 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
                         const bool act = own && (2 * d < mA || lane < d);
                         const int b = A0 + y;
                         const PGrad<S> gb = pair(act, b);
-                        if (act) pgrad_add(W.gr[b], gb);
+                        if (act) pgrad_add_at(W, b, gb);
                         __syncwarp();
                     }
                 }
@@ -1485,19 +1533,23 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
                             const bool act = own && y < mB;
                             const int b = B0 + (y < mB ? y : 0);
                             const PGrad<S> gb = pair(act, b);
-                            if (act) pgrad_add(W.gr[b], gb);
+                            if (act) pgrad_add_at(W, b, gb);
                             __syncwarp();
                         }
                     } else {
                         for (int y = 0; y < mB; ++y) {
                             const int b = B0 + y;
-                            pgrad_add_warp(W.gr[b], pair(own, b), lane);
+                            pgrad_add_warp(W, b, pair(own, b), lane);
                             __syncwarp();
                         }
                     }
                 }
                 // merge the own accumulator into its slot
-                if (own) acc.merge(W.gr[a]);
+                if (own) {
+                    Grad<S> ga = W.grad(a);
+                    acc.merge(ga);
+                    W.set_grad(a, ga);
+                }
                 __syncwarp();
             }
             return amb;
@@ -1508,7 +1560,7 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
             // with the exact test
             cnt = cnt0;
             en = szero<S>();
-            for (int e = lane; e < Ms; e += 32) W.gr[e] = grad_zero<S>();
+            for (int e = lane; e < Ms; e += 32) W.set_grad(e, grad_zero<S>());
             __syncwarp();
             exact_form = true;
         }
@@ -1517,7 +1569,7 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
         // flush the slots; s's gradient is minus the sum of all slot gradients
         V3<Acc> gia = widen(vzero<S>());
         for (int e = lane; e < Ms; e += 32) {
-            const V3<Acc> ge = slot_gradient<S, Acc>(W.gr[e], W.sd[e]);
+            const V3<Acc> ge = slot_gradient<S, Acc>(W.grad(e), W.slot(e));
             atomic_out(outs, W.idx[e], ge);
             gia = gia + ge;
         }
