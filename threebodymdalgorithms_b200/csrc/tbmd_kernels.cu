@@ -157,9 +157,21 @@ __device__ __forceinline__ float to_float<Dual<float>>(Dual<float> v) { return v
 // ---------------------------------------------------------------------------------------------
 // AUTA sweep
 
+// Register bound of the sweeps: the mixed form at R = 4 must fit two blocks of 8 warps per SM (128
+// registers); left free, its energy variant took 174 and ran 8% slower on the batched C5 systems.
+// The other forms keep the compiler's own choice.
+template <class S, int R>
+struct SweepMinBlocks {
+    static constexpr int value = 1;
+};
+template <>
+struct SweepMinBlocks<float, 4> {
+    static constexpr int value = 2;
+};
+
 template <class S, int R, bool ENERGY, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_auta(int64_t n, Pos pos, Out out, double *energy_out, double nu_d,
-                                                    SweepWork work)
+__global__ void __launch_bounds__(WARPS * 32, (SweepMinBlocks<S, R>::value))
+    k_auta(int64_t n, Pos pos, Out out, double *energy_out, double nu_d, SweepWork work)
 {
     using Acc = typename Traits<S>::Acc;
     constexpr int JB = 32 * R;
