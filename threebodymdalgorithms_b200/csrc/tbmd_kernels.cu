@@ -1073,12 +1073,15 @@ cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, const
 // lane x owns slot A+x: its edge and its gradient accumulator live in registers.
 //   - pairs inside A: circular diagonals, pair (x, (x + d) mod m_A), d = 1 .. m_A/2 (on the half
 //     diagonal of an even m_A only x < m_A/2);
-//   - pairs A x B with a later block B: if B is nearly full, a rotation, pair (x, (x + t) & 31),
-//     t = 0..31; otherwise each slot of B in turn against all lanes.
-// In every warp step the partner slots are distinct, so partner gradients are added to their slot
-// with a plain shared-memory read-modify-write (one __syncwarp per step, no atomics); in the
-// broadcast steps the partner gradient is first summed over the warp.  The own-slot gradient stays
-// in registers.  At the end of an item each slot is flushed with one FP64 atomic.
+//   - pairs A x B with a later block B: a full B (the FP64 and adjoint forms: m_B >= 24) by a
+//     rotation, pair (x, (x + t) & 31), t = 0..31.  A short B in the mixed forces form: lanes in
+//     groups of m_B, lane j of each group meets (j + t) mod m_B at step t = 0..m_B-1; groups after
+//     the first add their partner shares to per-warp copies, summed into B's slots at the end.  In
+//     the other forms each slot of B in turn against all lanes (broadcast steps).
+// In every warp step the partner slots (and copies) are distinct, so partner gradients are added with
+// a plain shared-memory read-modify-write (one __syncwarp per step, no atomics); in the broadcast
+// steps the partner gradient is first summed over the warp.  The own-slot gradient stays in
+// registers.  At the end of an item each slot is flushed with one FP64 atomic.
 //
 // Cutoff test of the third edge: the reference's periodic formula (structs.hpp:106-115) on the third
 // edge the triplet math uses (FP32 in the mixed form, FP64 in the FP64 forms), or, when no list
@@ -1127,6 +1130,21 @@ template <>
 __device__ __forceinline__ Grad<double> grad_zero<double>()
 {
     return Grad<double>{0.0, 0.0, 0.0, 0.0};
+}
+// dst += src, component-wise (the mixed form's accumulators, whose w is the factored scalar)
+template <class S>
+__device__ __forceinline__ void grad_merge(Grad<S> &dst, const Grad<S> &src)
+{
+    dst.x += src.x;
+    dst.y += src.y;
+    dst.z += src.z;
+    dst.w += src.w;
+}
+template <class S>
+__device__ __forceinline__ Grad<S> grad_shfl_down(const Grad<S> &v, int off)
+{
+    return Grad<S>{__shfl_down_sync(0xffffffffu, v.x, off), __shfl_down_sync(0xffffffffu, v.y, off),
+                   __shfl_down_sync(0xffffffffu, v.z, off), __shfl_down_sync(0xffffffffu, v.w, off)};
 }
 template <class S>
 __device__ __forceinline__ void slot_add(Grad<S> &slot, V3<S> g)
@@ -1224,13 +1242,36 @@ __device__ __forceinline__ V3<double> slot_gradient<float, double>(const Grad<fl
                       fma(w, (double)e.z, (double)g.z)};
 }
 
+// Partner accumulators of the lane groups g >= 1 of a short block B (see the item loops): (g - 1) m_B + y
+// < 32 entries.
+constexpr int P3_COPIES = 32;
+
+// The mixed forces kernel keeps a slot's neighbour index in the unused w of its lo-edge record (the
+// bits of an int32 in a float), and spends the freed 512 bytes per warp on the P3_COPIES accumulators
+// of the group form of short blocks.  The other forms keep an index array and reduce the partner
+// shares of a short block over the warp (the group form took their C3 kernel from 0.684 to 0.717 ms
+// in FP64: 4 KB more shared memory per CTA).
+template <class S>
+struct IdxInLo {
+    static constexpr bool value = false;
+};
+template <>
+struct IdxInLo<float> {
+    static constexpr bool value = true;
+};
+
 template <class S>
 struct SlotLayout {
     // per-warp shared memory, [2 * P3_CHUNK] of each: edge hi + b (Slot4), edge lo (Slot4, mixed only),
-    // gradient accumulator (Grad), neighbour index
+    // gradient accumulator (Grad), neighbour index (unless IdxInLo); then, if IdxInLo, P3_COPIES
+    // gradient accumulators
     static constexpr bool mixed = HasLo<S>::value;
     static constexpr int nlo = mixed ? 1 : 0;
-    static constexpr size_t bytes_per_slot = (1 + nlo) * sizeof(Slot4<S>) + sizeof(Grad<S>) + sizeof(int32_t);
+    static constexpr bool copies = IdxInLo<S>::value;
+    static constexpr size_t bytes_per_slot =
+        (1 + nlo) * sizeof(Slot4<S>) + sizeof(Grad<S>) + (IdxInLo<S>::value ? 0 : sizeof(int32_t));
+    static constexpr size_t bytes_per_warp =
+        2 * P3_CHUNK * bytes_per_slot + (copies ? P3_COPIES * sizeof(Grad<S>) : 0);
 };
 
 
@@ -1239,11 +1280,31 @@ struct P3Warp {
     Slot4<S> *sd;  // hi edge + b
     Slot4<S> *sl;  // lo edge (mixed)
     Grad<S> *gr;   // gradient accumulators
-    int32_t *idx;
+    int32_t *idx;  // neighbour indices (unless IdxInLo)
+    Grad<S> *cp;   // [P3_COPIES] partner accumulators of lane groups >= 1 (if IdxInLo)
+    __device__ __forceinline__ int32_t index(int i) const
+    {
+        if constexpr (IdxInLo<S>::value)
+            return __float_as_int(sl[i].w);
+        else
+            return idx[i];
+    }
+    // stage slot i's lo edge and neighbour index
+    __device__ __forceinline__ void set_lo_index(int i, const V3<S> &l, int32_t t) const
+    {
+        if constexpr (IdxInLo<S>::value) {
+            sl[i] = Slot4<S>{l.x, l.y, l.z, __int_as_float(t)};
+        } else {
+            idx[i] = t;
+            if constexpr (HasLo<S>::value) sl[i] = Slot4<S>{l.x, l.y, l.z, szero<S>()};
+        }
+    }
     __device__ __forceinline__ Slot4<S> slot(int i) const { return sd[i]; }
     __device__ __forceinline__ void set_slot(int i, const Slot4<S> &v) const { sd[i] = v; }
     __device__ __forceinline__ Grad<S> grad(int i) const { return gr[i]; }
     __device__ __forceinline__ void set_grad(int i, const Grad<S> &v) const { gr[i] = v; }
+    __device__ __forceinline__ Grad<S> copy(int i) const { return cp[i]; }
+    __device__ __forceinline__ void set_copy(int i, const Grad<S> &v) const { cp[i] = v; }
 };
 // FP64: the 32-byte slot and accumulator records are stored as two arrays of 16-byte halves, (x, y)
 // for all slots and then (z, w), so that the 16-byte accesses of a warp to consecutive slots are free
@@ -1256,6 +1317,9 @@ struct P3Warp<double> {
     Slot4<double> *sl;  // unused
     Grad<double> *gr;   // [SL] (x, y), then [SL] (z, w), as double2
     int32_t *idx;
+    Grad<double> *cp;   // unused
+    __device__ __forceinline__ int32_t index(int i) const { return idx[i]; }
+    __device__ __forceinline__ void set_lo_index(int i, const V3<double> &, int32_t t) const { idx[i] = t; }
     __device__ __forceinline__ Slot4<double> slot(int i) const
     {
         const double2 a = ((const double2 *)sd)[i], b = ((const double2 *)sd)[SL + i];
@@ -1277,13 +1341,20 @@ struct P3Warp<double> {
         ((double2 *)gr)[SL + i] = make_double2(v.z, v.w);
     }
 };
-// read-modify-write of slot i's accumulator with a partner share
+// read-modify-write of slot i's accumulator (or of copy i) with a partner share
 template <class S>
 __device__ __forceinline__ void pgrad_add_at(const P3Warp<S> &W, int i, const PGrad<S> &pg)
 {
     Grad<S> g = W.grad(i);
     pgrad_add(g, pg);
     W.set_grad(i, g);
+}
+template <class S>
+__device__ __forceinline__ void pgrad_add_copy(const P3Warp<S> &W, int i, const PGrad<S> &pg)
+{
+    Grad<S> g = W.copy(i);
+    pgrad_add(g, pg);
+    W.set_copy(i, g);
 }
 // partner shares of all lanes for one common partner slot, added by lane 0
 template <class S>
@@ -1340,7 +1411,7 @@ __device__ __forceinline__ bool cut_inside(const P3Warp<S> &W, const CellBufs &c
         }
         if (d2 <= sq_lo) return true;
         if (d2 > sq_hi) return false;
-        const int32_t ta = W.idx[a], tb = W.idx[b];
+        const int32_t ta = W.index(a), tb = W.index(b);
         return sqdist_periodic(cb.xs[ta], cb.ys[ta], cb.zs[ta], cb.xs[tb], cb.ys[tb], cb.zs[tb], g) <= g.sqcut;
     }
     // FP64 forms: the same guarded test in FP64 on the FP64 third edge, with the FP64 band
@@ -1354,7 +1425,7 @@ __device__ __forceinline__ bool cut_inside(const P3Warp<S> &W, const CellBufs &c
     }
     if (d2 <= g.sqcut - g.band64) return true;
     if (d2 > g.sqcut + g.band64) return false;
-    const int32_t ta = W.idx[a], tb = W.idx[b];
+    const int32_t ta = W.index(a), tb = W.index(b);
     return sqdist_periodic(cb.xs[ta], cb.ys[ta], cb.zs[ta], cb.xs[tb], cb.ys[tb], cb.zs[tb], g) <= g.sqcut;
 }
 
@@ -1397,12 +1468,15 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
     const int cap = cb.cap;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    unsigned char *base = smem + (size_t)wib * SL * L::bytes_per_slot;
+    unsigned char *base = smem + (size_t)wib * L::bytes_per_warp;
     P3Warp<S> W;
     W.sd = (Slot4<S> *)base;
     W.sl = W.sd + SL;
     W.gr = (Grad<S> *)(W.sl + (L::nlo ? SL : 0));
-    W.idx = (int32_t *)(W.gr + SL);
+    W.idx = IdxInLo<S>::value ? nullptr : (int32_t *)(W.gr + SL);
+    W.cp = L::copies ? W.gr + SL : nullptr;
+    if constexpr (L::copies) W.set_copy(lane, grad_zero<S>());
+    __syncwarp();
 
     const S nu = constant<S>(nu_d), nu3 = constant<S>(-3.0 * nu_d), nu15 = constant<S>(15.0 * nu_d);
     const Out outs = {cb.fs[0], cb.fs[1], cb.fs[2], cb.hs[0], cb.hs[1], cb.hs[2]};
@@ -1443,7 +1517,6 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
         for (int e = lane; e < Ms; e += 32) {
             const int pos_in_list = e < mI ? offI + e : offJ + (e - mI);
             const int32_t t = (int32_t)TBMD_IX(cb.nbr[(int64_t)s * cap + pos_in_list], n, BS_LIST);
-            W.idx[e] = t;
             const double x = cb.xs[t], y = cb.ys[t], z = cb.zs[t];
             const double ddx = x - xi, ddy = y - yi, ddz = z - zi;
             nowrap = nowrap && fabs(ddx) <= cwrap && fabs(ddy) <= cwrap && fabs(ddz) <= cwrap;
@@ -1452,7 +1525,7 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
             split<S>(ddy, dual ? cb.dys[t] - dyi : 0.0, v.y, l.y);
             split<S>(ddz, dual ? cb.dzs[t] - dzi : 0.0, v.z, l.z);
             W.set_slot(e, Slot4<S>{v.x, v.y, v.z, dot3(v, v)});
-            if (L::nlo) W.sl[e] = Slot4<S>{l.x, l.y, l.z, szero<S>()};
+            W.set_lo_index(e, l, t);
             W.set_grad(e, grad_zero<S>());
         }
         const bool rawok = G.raw_ok && __all_sync(0xffffffffu, nowrap);
@@ -1539,7 +1612,10 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
                 // pairs A x B with every later block B (of the same chunk, or of the second chunk)
                 for (int B0 = (mJ == 0 ? A0 + 32 : mI); B0 < Ms; B0 += 32) {
                     const int mB = min(32, Ms - B0);
-                    if (mB >= 24) {
+                    // a full block: 32 steps of distinct partners.  A short block takes mB steps in
+                    // lane groups (the mixed form) or broadcast steps with a warp reduction of the
+                    // partner share (the others, for mB < 24, where that beats 32 partly idle steps)
+                    if (mB >= (L::copies ? 32 : 24)) {
                         for (int t = 0; t < 32; ++t) {
                             const int y = (lane + t) & 31;
                             const bool act = own && y < mB;
@@ -1548,6 +1624,38 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
                             if (act) pgrad_add_at(W, b, gb);
                             __syncwarp();
                         }
+                    } else if constexpr (L::copies) {
+                        // a short block: lanes form groups of mB, and lane j of group g meets partner
+                        // (j + t) mod mB at step t, so the partners of one group are distinct.  Group 0
+                        // adds to B's slots and group g >= 1 to copy (g - 1) mB + y.  Then lane l takes
+                        // copy l (partner l mod mB), and the copies of a partner sum down the lanes
+                        // l, l + mB, l + 2 mB, ... into lane l < mB.
+                        const int g = lane / mB, j = lane - g * mB;
+                        int y = j;
+                        for (int t = 0; t < mB; ++t) {
+                            const int b = B0 + y;
+                            const PGrad<S> gb = pair(own, b);
+                            if (own) {
+                                if (g == 0)
+                                    pgrad_add_at(W, b, gb);
+                                else
+                                    pgrad_add_copy(W, (int)TBMD_IX((g - 1) * mB + y, P3_COPIES, BS_SLOT), gb);
+                            }
+                            __syncwarp();
+                            y = y + 1 == mB ? 0 : y + 1;
+                        }
+                        Grad<S> c = W.copy(lane);
+                        W.set_copy(lane, grad_zero<S>());
+                        for (int off = mB; off < 32; off *= 2) {
+                            const Grad<S> o = grad_shfl_down(c, off);
+                            if (lane + off < 32) grad_merge(c, o);
+                        }
+                        if (lane < mB) {
+                            Grad<S> gl = W.grad(B0 + lane);
+                            grad_merge(gl, c);
+                            W.set_grad(B0 + lane, gl);
+                        }
+                        __syncwarp();
                     } else {
                         for (int y = 0; y < mB; ++y) {
                             const int b = B0 + y;
@@ -1582,7 +1690,7 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
         V3<Acc> gia = widen(vzero<S>());
         for (int e = lane; e < Ms; e += 32) {
             const V3<Acc> ge = slot_gradient<S, Acc>(W.grad(e), W.slot(e));
-            atomic_out(outs, W.idx[e], ge);
+            atomic_out(outs, W.index(e), ge);
             gia = gia + ge;
         }
         gia = warp_sum3(gia);
@@ -1680,7 +1788,7 @@ static cudaError_t plan_p3bca_t(bool energy, int cap, int warps, P3Plan *plan)
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     (void)cap;
-    const size_t per_warp = (size_t)2 * P3_CHUNK * SlotLayout<S>::bytes_per_slot;
+    const size_t per_warp = SlotLayout<S>::bytes_per_warp;
     const size_t smem_cap = 220 * 1024;
     if (warps < 1) warps = 1;
     if (warps > 8) warps = 8;
