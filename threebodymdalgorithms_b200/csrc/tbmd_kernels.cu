@@ -1146,6 +1146,13 @@ __device__ __forceinline__ Grad<S> grad_shfl_down(const Grad<S> &v, int off)
     return Grad<S>{__shfl_down_sync(0xffffffffu, v.x, off), __shfl_down_sync(0xffffffffu, v.y, off),
                    __shfl_down_sync(0xffffffffu, v.z, off), __shfl_down_sync(0xffffffffu, v.w, off)};
 }
+template <>
+__device__ __forceinline__ Grad<double> grad_shfl_down<double>(const Grad<double> &v, int off)
+{
+    // w is padding in the FP64 accumulators
+    return Grad<double>{__shfl_down_sync(0xffffffffu, v.x, off), __shfl_down_sync(0xffffffffu, v.y, off),
+                        __shfl_down_sync(0xffffffffu, v.z, off), 0.0};
+}
 template <class S>
 __device__ __forceinline__ void slot_add(Grad<S> &slot, V3<S> g)
 {
@@ -1247,16 +1254,28 @@ __device__ __forceinline__ V3<double> slot_gradient<float, double>(const Grad<fl
 constexpr int P3_COPIES = 32;
 
 // The mixed forces kernel keeps a slot's neighbour index in the unused w of its lo-edge record (the
-// bits of an int32 in a float), and spends the freed 512 bytes per warp on the P3_COPIES accumulators
-// of the group form of short blocks.  The other forms keep an index array and reduce the partner
-// shares of a short block over the warp (the group form took their C3 kernel from 0.684 to 0.717 ms
-// in FP64: 4 KB more shared memory per CTA).
+// bits of an int32 in a float), so that the P3_COPIES accumulators of the group form of short blocks
+// fit in the shared memory of 8 CTAs per SM.  The FP64 forces kernel, whose occupancy its registers
+// bound, keeps its index array and adds the copies.  The adjoint forms reduce the partner shares of a
+// short block over the warp (broadcast steps).
 template <class S>
 struct IdxInLo {
     static constexpr bool value = false;
 };
 template <>
 struct IdxInLo<float> {
+    static constexpr bool value = true;
+};
+template <class S>
+struct GroupCopies {
+    static constexpr bool value = false;
+};
+template <>
+struct GroupCopies<float> {
+    static constexpr bool value = true;
+};
+template <>
+struct GroupCopies<double> {
     static constexpr bool value = true;
 };
 
@@ -1267,7 +1286,7 @@ struct SlotLayout {
     // gradient accumulators
     static constexpr bool mixed = HasLo<S>::value;
     static constexpr int nlo = mixed ? 1 : 0;
-    static constexpr bool copies = IdxInLo<S>::value;
+    static constexpr bool copies = GroupCopies<S>::value;
     static constexpr size_t bytes_per_slot =
         (1 + nlo) * sizeof(Slot4<S>) + sizeof(Grad<S>) + (IdxInLo<S>::value ? 0 : sizeof(int32_t));
     static constexpr size_t bytes_per_warp =
@@ -1317,8 +1336,18 @@ struct P3Warp<double> {
     Slot4<double> *sl;  // unused
     Grad<double> *gr;   // [SL] (x, y), then [SL] (z, w), as double2
     int32_t *idx;
-    Grad<double> *cp;   // unused
+    Grad<double> *cp;   // [P3_COPIES] (x, y), then [P3_COPIES] (z, w), as double2
     __device__ __forceinline__ int32_t index(int i) const { return idx[i]; }
+    __device__ __forceinline__ Grad<double> copy(int i) const
+    {
+        const double2 a = ((const double2 *)cp)[i], b = ((const double2 *)cp)[P3_COPIES + i];
+        return Grad<double>{a.x, a.y, b.x, b.y};
+    }
+    __device__ __forceinline__ void set_copy(int i, const Grad<double> &v) const
+    {
+        ((double2 *)cp)[i] = make_double2(v.x, v.y);
+        ((double2 *)cp)[P3_COPIES + i] = make_double2(v.z, v.w);
+    }
     __device__ __forceinline__ void set_lo_index(int i, const V3<double> &, int32_t t) const { idx[i] = t; }
     __device__ __forceinline__ Slot4<double> slot(int i) const
     {
@@ -1444,8 +1473,8 @@ struct P3MaxReg<float, true> {
     static constexpr int value = 72;
 };
 template <bool E>
-struct P3MaxReg<double, E> {  // 88: 3.8% faster at C3 than 80 (fewer spills; 22 resident warps instead of 24)
-    static constexpr int value = 88;
+struct P3MaxReg<double, E> {  // 96 with the group form (0.701 ms at C3; 88 spills 96 B, 104 is 0.733 ms)
+    static constexpr int value = 96;
 };
 template <bool E>
 struct P3MaxReg<Dual<float>, E> {
@@ -1474,7 +1503,7 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
     W.sl = W.sd + SL;
     W.gr = (Grad<S> *)(W.sl + (L::nlo ? SL : 0));
     W.idx = IdxInLo<S>::value ? nullptr : (int32_t *)(W.gr + SL);
-    W.cp = L::copies ? W.gr + SL : nullptr;
+    W.cp = !L::copies ? nullptr : IdxInLo<S>::value ? W.gr + SL : (Grad<S> *)(W.idx + SL);
     if constexpr (L::copies) W.set_copy(lane, grad_zero<S>());
     __syncwarp();
 
