@@ -791,12 +791,13 @@ cudaError_t launch_unsort_update(int64_t n, const CellBufs &cb, double *const st
 // particle s in c are: the particles of c after s, and all particles of the neighbour cells with
 // id > c.  nbr_cells (built on the host with the grid) lists, per cell, its neighbour cells with
 // id >= c in increasing id order (-1 padded to 27).  The block scans their sizes and stages their
-// particles (FP32 hi/lo positions relative to the box corner, and sorted indices) in shared memory
-// in that order - cell by cell, so every copy is coalesced - and the candidates of the i-th
-// particle of c are the suffix after i.  Warps take the particles of c in turn and sweep their
-// suffix 32 candidates at a time, writing survivors compacted by ballot.  A cell whose candidates
-// exceed the staging capacity reads them from global memory instead.  Lists longer than cap are
-// truncated; the largest length is recorded so the host can enlarge cap and recompute.
+// particles (FP32 hi/lo positions relative to the box corner, with the sorted index in the hi
+// record's spare w) in shared memory in that order - cell by cell, so every copy is coalesced - and
+// the candidates of the i-th particle of c are the suffix after i.  Warps take the particles of c in
+// turn and sweep their suffix 32 candidates at a time, writing survivors compacted by ballot.  A
+// cell whose candidates exceed the staging capacity reads them from global memory instead.  Lists
+// longer than cap are truncated; the largest length is recorded so the host can enlarge cap and
+// recompute.
 //
 // The test runs in FP32 on d = (hi_t - hi_s) + (lo_t - lo_s), which is within 2^-24 (|d| + L) of
 // the FP64 difference per component, inside the bound e = 16 eps32 (L + cutoff) of the guard band
@@ -809,7 +810,7 @@ cudaError_t launch_unsort_update(int64_t n, const CellBufs &cb, double *const st
 // 2 cells <= L / 2 per axis: there the periodic form equals the raw distance and the hi parts alone
 // are accurate to 2^-24 L, so the cheaper test is used.  Elsewhere min(|d|, L - |d|) on hi + lo.
 constexpr int NB_THREADS = 128;
-constexpr size_t NB_STAGE_BYTES = 2 * sizeof(float4) + sizeof(int32_t);  // per staged candidate
+constexpr size_t NB_STAGE_BYTES = 2 * sizeof(float4);  // per staged candidate (hi with the index in w, lo)
 
 __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(int64_t n, const __grid_constant__ Grid g, GridSet set,
                                                           const int32_t *__restrict__ nbr_cells,
@@ -828,7 +829,6 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(int64_t n, const _
     extern __shared__ __align__(16) unsigned char smraw[];
     float4 *shi = (float4 *)smraw;
     float4 *slo = shi + max_stage;
-    int32_t *st = (int32_t *)(slo + max_stage);
     __shared__ int cstart[32], cpre[33], raw_cell;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int NW = NB_THREADS / 32;
@@ -888,13 +888,13 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(int64_t n, const _
                     const int k = entry_of(q);
                     const int t = (int)TBMD_IX(cstart[k] + (q - cpre[k]), n, BS_CANDIDATE);
                     (void)TBMD_IX(q, max_stage, BS_STAGE);
-                    shi[q] = qhi[t];
+                    float4 h = qhi[t];
+                    h.w = __int_as_float(t);  // the sorted index rides in the unused w
+                    shi[q] = h;
                     slo[q] = qlo[t];
-                    st[q] = t;
                 } else {
-                    shi[q] = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+                    shi[q] = make_float4(1e18f, 1e18f, 1e18f, __int_as_float(-1));
                     slo[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    st[q] = -1;
                 }
             }
         }
@@ -925,7 +925,7 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(int64_t n, const _
                 for (int q0 = sl + 1; q0 < T; q0 += 32) {
                     const int q = q0 + lane;
                     const float4 h = shi[q];
-                    const int t = st[q];
+                    const int t = __float_as_int(h.w);
                     const float dx = h.x - oh.x, dy = h.y - oh.y, dz = h.z - oh.z;
                     const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                     bool pass = d2 <= sq_lo;
@@ -936,7 +936,7 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(int64_t n, const _
                 for (int q0 = sl + 1; q0 < T; q0 += 32) {
                     const int q = q0 + lane;
                     const float4 h = shi[q], l = slo[q];
-                    const int t = st[q];
+                    const int t = __float_as_int(h.w);
                     const float dx = (h.x - oh.x) + (l.x - ol.x), dy = (h.y - oh.y) + (l.y - ol.y),
                                 dz = (h.z - oh.z) + (l.z - ol.z);
                     const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
