@@ -441,6 +441,51 @@ def test_clustered_capacity_retry():
     ctx.close()
 
 
+def converging_lattice(m=13, k=40.0, seed=7):
+    """m^3 particles on a jittered cubic lattice at density 2.048 (no close pairs), moving towards the
+    centre with velocity -k (x - centre)."""
+    rng = np.random.default_rng(seed)
+    a = (1 / 2.048) ** (1 / 3)
+    idx = np.stack(np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij"), -1).reshape(-1, 3)
+    x = (idx + 0.5) * a + rng.uniform(-0.1, 0.1, idx.shape)
+    n = len(x)
+    st = {"x": x[:, 0].copy(), "y": x[:, 1].copy(), "z": x[:, 2].copy(), "m": np.ones(n),
+          "id": np.arange(n, dtype=np.int32)}
+    for i, v in enumerate(("vx", "vy", "vz")):
+        st[v] = -k * (x[:, i] - x[:, i].mean())
+    for f in ("ax", "ay", "az"):
+        st[f] = np.zeros(n)
+    return st
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_overflow_inside_a_multi_step_call(prec):
+    """A converging lattice: its half lists fit the mean-density capacity (160) at the first steps and
+    outgrow it at about the eighth of a 10-step call.  The call is re-run from its snapshot with
+    larger lists (the triplet kernel skips its work for the rest of the attempt that overflowed),
+    and the result is the oracle's.  The grown capacity is kept, so the same call again runs once."""
+    st = converging_lattice()
+    ref, counts = O.simulate("p3bca", 10, st, 0.001, (0.0, -9.81, 0.0), cutoff=2.0, nthreads=0)
+    assert counts[-1] > 1.5 * counts[0]  # the lattice compresses
+    ctx = Context("p3bca", prec, 2.0, 0.001, (0.0, -9.81, 0.0))
+    runs = []
+    for _ in range(2):
+        ctx.set_state(st)
+        k0 = ctx.kernel_launches()
+        c = ctx.step(10)
+        runs.append((c, ctx.get_state(), ctx.kernel_launches() - k0))
+    ctx.close()
+    assert runs[0][2] > runs[1][2]  # the first call ran its steps twice
+    for c, got, _ in runs:
+        if prec == "fp64":
+            assert np.array_equal(c, counts)
+            check_state(got, ref, FP64_MULTISTEP_FORCE_TOL, FP64_MULTISTEP_TOL)
+        else:
+            assert counts_close(c, counts, 1e-3), (c, counts)
+            for k in ("x", "y", "z"):
+                assert rel_l2(got[k], ref[k]) <= MIXED_MULTISTEP_POS_TOL, k
+
+
 @pytest.mark.parametrize("n", [1, 2])
 def test_fewer_than_three_particles(n):
     st = generators.uniform(n, (3, 3, 3))

@@ -578,41 +578,72 @@ __global__ void k_cell_assign(int64_t n, const double *__restrict__ x, const dou
     if (out) cell_out[c] = 1;
 }
 
-// Exclusive scan of cell counts (single block of 1024 threads, each owning a contiguous chunk; the
-// chunk totals are scanned with warp shuffles, then across the 32 warps).
+// Exclusive scan of cell counts: one block of 1024 threads over tiles of 8192 cells.  A tile is read
+// into shared memory with coalesced loads (all issued before the first is used), each thread scans
+// its 8 contiguous cells there, the thread totals are scanned with warp shuffles and across the 32
+// warps, and the starts go back out with coalesced stores.  A carry links the tiles.
+constexpr int SCAN_PER_THREAD = 8;
+
 __global__ void __launch_bounds__(1024) k_cell_scan(int64_t ncells, const int32_t *__restrict__ count,
                                                     int32_t *__restrict__ start)
 {
+    constexpr int TILE = 1024 * SCAN_PER_THREAD;
+    __shared__ __align__(16) int32_t tile[TILE];
     __shared__ int32_t wsum[32];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int64_t chunk = (ncells + 1023) / 1024;
-    const int64_t b = t * chunk, e = (b + chunk < ncells) ? b + chunk : ncells;
-    int32_t s = 0;
-    for (int64_t c = b; c < e; ++c) s += count[c];
-    int32_t inc = s;
+    int32_t carry = 0;
+    for (int64_t base = 0; base < ncells; base += TILE) {
+        const int m = (int)(ncells - base < TILE ? ncells - base : TILE);
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int32_t v = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += v;
-    }
-    if (lane == 31) wsum[warp] = inc;
-    __syncthreads();
-    if (warp == 0) {
-        int32_t w = wsum[lane];
+        for (int k = 0; k < SCAN_PER_THREAD; ++k) {
+            const int i = k * 1024 + t;
+            tile[i] = i < m ? count[base + i] : 0;
+        }
+        __syncthreads();
+        const int4 *own = (const int4 *)(tile + t * SCAN_PER_THREAD);
+        const int4 p = own[0], q = own[1];
+        const int32_t v[SCAN_PER_THREAD] = {p.x, p.y, p.z, p.w, q.x, q.y, q.z, q.w};
+        int32_t s = 0;
+#pragma unroll
+        for (int k = 0; k < SCAN_PER_THREAD; ++k) s += v[k];
+        int32_t inc = s;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int32_t v = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += v;
+            const int32_t x = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += x;
         }
-        wsum[lane] = w;  // inclusive over warps
+        if (lane == 31) wsum[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            int32_t w = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t x = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += x;
+            }
+            wsum[lane] = w;  // inclusive over warps
+        }
+        __syncthreads();
+        int32_t run = carry + (warp > 0 ? wsum[warp - 1] : 0) + inc - s;
+        int32_t ex[SCAN_PER_THREAD];
+#pragma unroll
+        for (int k = 0; k < SCAN_PER_THREAD; ++k) {
+            ex[k] = run;
+            run += v[k];
+        }
+        int4 *own_w = (int4 *)(tile + t * SCAN_PER_THREAD);
+        own_w[0] = make_int4(ex[0], ex[1], ex[2], ex[3]);
+        own_w[1] = make_int4(ex[4], ex[5], ex[6], ex[7]);
+        carry += wsum[31];
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < SCAN_PER_THREAD; ++k) {
+            const int i = k * 1024 + t;
+            if (i < m) start[base + i] = tile[i];
+        }
+        __syncthreads();  // the tile and wsum are reused by the next tile
     }
-    __syncthreads();
-    int32_t run = (warp > 0 ? wsum[warp - 1] : 0) + inc - s;
-    for (int64_t c = b; c < e; ++c) {
-        start[c] = run;
-        run += count[c];
-    }
-    if (t == 1023) start[ncells] = wsum[31];
+    if (t == 0) start[ncells] = carry;
 }
 
 __global__ void k_cell_scatter(int64_t n, const int32_t *__restrict__ cell_of, const int32_t *__restrict__ start,
@@ -810,6 +841,9 @@ cudaError_t launch_unsort_update(int64_t n, const CellBufs &cb, double *const st
 // 2 cells <= L / 2 per axis: there the periodic form equals the raw distance and the hi parts alone
 // are accurate to 2^-24 L, so the cheaper test is used.  Elsewhere min(|d|, L - |d|) on hi + lo.
 constexpr int NB_THREADS = 128;
+// Start value of the triplet kernel's work counters that leaves it nothing to do: above every particle
+// and item index (both below 2^31), with room for one increment per warp.
+constexpr unsigned int P3_NO_WORK = 0x80000000u;
 constexpr size_t NB_STAGE_BYTES = 2 * sizeof(float4);  // per staged candidate (hi with the index in w, lo)
 
 __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(int64_t n, const __grid_constant__ Grid g, GridSet set,
@@ -824,8 +858,17 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(int64_t n, const _
                                                           int32_t *nbr_count, int32_t *max_count, int cap,
                                                           int max_stage, unsigned long long *long_items,
                                                           unsigned int long_cap, unsigned int *long_count,
-                                                          unsigned int *long_max)
+                                                          unsigned int *long_max, unsigned int *work_counter)
 {
+    // Arm the triplet kernel's two work counters (it runs next on the stream).  After a list or
+    // chunk-pair overflow in an earlier step of the same call (the flags are cleared per call and
+    // only grow) the host re-runs the call with larger capacities and drops what the steps compute,
+    // so the counters start past every item and the triplet kernel of this step does no work.
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const bool over = *(volatile int32_t *)max_count > cap || *(volatile unsigned int *)long_max > long_cap;
+        work_counter[0] = over ? P3_NO_WORK : 0u;
+        work_counter[1] = over ? P3_NO_WORK : 0u;
+    }
     extern __shared__ __align__(16) unsigned char smraw[];
     float4 *shi = (float4 *)smraw;
     float4 *slo = shi + max_stage;
@@ -1056,7 +1099,7 @@ cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, const
                                                             cb.cell_start, cb.cell_out, cb.nbr, cb.nbr_count,
                                                             cb.max_count, cb.cap,
                                                             max_stage, cb.long_items, (unsigned int)cb.long_cap,
-                                                            cb.long_count, cb.long_max);
+                                                            cb.long_count, cb.long_max, cb.work_counter);
     return cudaGetLastError();
 }
 
@@ -1854,8 +1897,7 @@ template <class S>
 static cudaError_t launch_p3bca_t(bool energy, int64_t n, const Grid &g, const GridSet &set, CellBufs &cb, double nu,
                                   double *eo, unsigned long long *co, const P3Plan &plan, cudaStream_t st)
 {
-    cudaError_t e;
-    if ((e = cudaMemsetAsync(cb.work_counter, 0, 2 * sizeof(unsigned int), st)) != cudaSuccess) return e;
+    // the work counters were armed by the neighbour kernel of the same step
     auto kern = energy ? k_p3bca<S, true> : k_p3bca<S, false>;
     kern<<<plan.grid, plan.warps * 32, plan.smem, st>>>(n, g, set, cb, nu, eo, co);
     return cudaGetLastError();
