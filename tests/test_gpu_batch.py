@@ -48,12 +48,11 @@ def test_batch_forces_match_single_systems(algo, cutoff, precision, tol):
         got = np.stack([fx[sl], fy[sl], fz[sl]], 1)
         assert rel_l2(got, ref) <= tol, (s, rel_l2(got, ref))
         e_ref = O.energy(st["x"], st["y"], st["z"], 1.0, cutoff if cutoff > 0 else -1.0, L, lo)
-        if precision == "fp64":
-            assert abs(energy[s] - e_ref) <= 1e-12 * max(abs(e_ref), 1e-30)
-        else:
-            # relative to the magnitude scale of the terms, which have both signs (see test_gpu_parity)
-            e_abs = O.energy_abs(st["x"], st["y"], st["z"], 1.0, cutoff if cutoff > 0 else -1.0, L, lo)
-            assert abs(energy[s] - e_ref) <= 2e-6 * max(e_abs, 1e-30), (s, energy[s], e_ref, e_abs)
+        # relative to the magnitude scale of the terms, which have both signs (see test_gpu_parity):
+        # the FP64 sum's order follows the device's atomics, so its rounding is bounded by that scale
+        e_abs = O.energy_abs(st["x"], st["y"], st["z"], 1.0, cutoff if cutoff > 0 else -1.0, L, lo)
+        etol = 1e-12 if precision == "fp64" else 2e-6
+        assert abs(energy[s] - e_ref) <= etol * max(e_abs, 1e-30), (s, energy[s], e_ref, e_abs)
     ctx.close()
 
 

@@ -1771,33 +1771,67 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
         __syncwarp();
     };
 
-    // lists of at most one chunk: one item per particle
-    unsigned int w = 0;
-    if (lane == 0) w = atomicAdd(cb.work_counter, 1u);
-    w = __shfl_sync(0xffffffffu, w, 0);
-    while ((int64_t)w < n) {
-        unsigned int wn = 0;
-        if (lane == 0) wn = atomicAdd(cb.work_counter, 1u);
-        const int s = (int)w;
-        const int M = min(cb.nbr_count[s], cap);
-        if (M <= P3_CHUNK && M > 1) item(s, 0, M, 0, 0);
-        w = __shfl_sync(0xffffffffu, wn, 0);
-    }
-    // longer lists: the chunk-pair items the neighbour kernel queued
-    const unsigned int nlong = min(*cb.long_count, (unsigned int)cb.long_cap);
-    if (lane == 0) w = atomicAdd(cb.work_counter + 1, 1u);
-    w = __shfl_sync(0xffffffffu, w, 0);
-    while (w < nlong) {
-        unsigned int wn = 0;
-        if (lane == 0) wn = atomicAdd(cb.work_counter + 1, 1u);
-        const unsigned long long it = cb.long_items[w];
-        const int s = (int)TBMD_IX((int64_t)(it >> 32), n, BS_LONG_ITEM), I = (int)((it >> 16) & 0xffffu),
-                  J = (int)(it & 0xffffu);
-        const int M = min(cb.nbr_count[s], cap);
-        const int mI = min(P3_CHUNK, M - I * P3_CHUNK);
-        const int mJ = J != I ? min(P3_CHUNK, M - J * P3_CHUNK) : 0;
-        item(s, I * P3_CHUNK, mI, J * P3_CHUNK, mJ);
-        w = __shfl_sync(0xffffffffu, wn, 0);
+    if constexpr (Traits<S>::dual) {
+        // the dual forms run both kinds of item through one call site, which lets the compiler inline
+        // the item (two call sites left it an out-of-line function with a large stack frame)
+        for (int kind = 0; kind < 2; ++kind) {
+            const unsigned int lim = kind == 0 ? (unsigned int)n : min(*cb.long_count, (unsigned int)cb.long_cap);
+            unsigned int w = 0;
+            if (lane == 0) w = atomicAdd(cb.work_counter + kind, 1u);
+            w = __shfl_sync(0xffffffffu, w, 0);
+            while (w < lim) {
+                unsigned int wn = 0;
+                if (lane == 0) wn = atomicAdd(cb.work_counter + kind, 1u);
+                int s, offI = 0, mI, offJ = 0, mJ = 0;
+                if (kind == 0) {
+                    s = (int)w;
+                    mI = min(cb.nbr_count[s], cap);
+                    if (mI > P3_CHUNK) mI = 0;  // a long list: its chunk pairs come as items of kind 1
+                } else {
+                    const unsigned long long it = cb.long_items[w];
+                    s = (int)TBMD_IX((int64_t)(it >> 32), n, BS_LONG_ITEM);
+                    const int I = (int)((it >> 16) & 0xffffu), J = (int)(it & 0xffffu);
+                    const int M = min(cb.nbr_count[s], cap);
+                    offI = I * P3_CHUNK;
+                    mI = min(P3_CHUNK, M - offI);
+                    if (J != I) {
+                        offJ = J * P3_CHUNK;
+                        mJ = min(P3_CHUNK, M - offJ);
+                    }
+                }
+                if (mI + mJ > 1) item(s, offI, mI, offJ, mJ);
+                w = __shfl_sync(0xffffffffu, wn, 0);
+            }
+        }
+    } else {
+        // lists of at most one chunk: one item per particle
+        unsigned int w = 0;
+        if (lane == 0) w = atomicAdd(cb.work_counter, 1u);
+        w = __shfl_sync(0xffffffffu, w, 0);
+        while ((int64_t)w < n) {
+            unsigned int wn = 0;
+            if (lane == 0) wn = atomicAdd(cb.work_counter, 1u);
+            const int s = (int)w;
+            const int M = min(cb.nbr_count[s], cap);
+            if (M <= P3_CHUNK && M > 1) item(s, 0, M, 0, 0);
+            w = __shfl_sync(0xffffffffu, wn, 0);
+        }
+        // longer lists: the chunk-pair items the neighbour kernel queued
+        const unsigned int nlong = min(*cb.long_count, (unsigned int)cb.long_cap);
+        if (lane == 0) w = atomicAdd(cb.work_counter + 1, 1u);
+        w = __shfl_sync(0xffffffffu, w, 0);
+        while (w < nlong) {
+            unsigned int wn = 0;
+            if (lane == 0) wn = atomicAdd(cb.work_counter + 1, 1u);
+            const unsigned long long it = cb.long_items[w];
+            const int s = (int)TBMD_IX((int64_t)(it >> 32), n, BS_LONG_ITEM), I = (int)((it >> 16) & 0xffffu),
+                      J = (int)(it & 0xffffu);
+            const int M = min(cb.nbr_count[s], cap);
+            const int mI = min(P3_CHUNK, M - I * P3_CHUNK);
+            const int mJ = J != I ? min(P3_CHUNK, M - J * P3_CHUNK) : 0;
+            item(s, I * P3_CHUNK, mI, J * P3_CHUNK, mJ);
+            w = __shfl_sync(0xffffffffu, wn, 0);
+        }
     }
     flush(cur_sys);
 }
