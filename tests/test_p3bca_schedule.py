@@ -26,11 +26,10 @@ def diagonal_steps(A0, mA):
         yield step
 
 
-def cross_steps(A0, mA, B0, mB, group_form):
-    """Pairs A x B.  A full B: a rotation (x, (x + t) & 31).  A short B in the group form: lane j of group
-    g meets (j + t) mod m_B at step t; group 0 adds to B's slots, group g >= 1 to copy (g - 1) m_B + y.
-    Otherwise broadcast steps: slot B0 + y against all lanes, summed over the warp first."""
-    if mB >= (32 if group_form else 24):
+def cross_steps(A0, mA, B0, mB):
+    """Pairs A x B.  A full B: a rotation (x, (x + t) & 31).  A short B: lane j of group g meets
+    (j + t) mod m_B at step t; group 0 adds to B's slots, group g >= 1 to copy (g - 1) m_B + y."""
+    if mB == 32:
         for t in range(32):
             step = []
             for lane in range(mA):
@@ -38,7 +37,7 @@ def cross_steps(A0, mA, B0, mB, group_form):
                 if y < mB:
                     step.append((A0 + lane, B0 + y, ("slot", B0 + y)))
             yield step
-    elif group_form:
+    else:
         for t in range(mB):
             step = []
             for lane in range(mA):
@@ -47,13 +46,9 @@ def cross_steps(A0, mA, B0, mB, group_form):
                 tgt = ("slot", B0 + y) if g == 0 else ("copy", (g - 1) * mB + y)
                 step.append((A0 + lane, B0 + y, tgt))
             yield step
-    else:
-        for y in range(mB):
-            # one warp-reduced add to slot B0 + y
-            yield [(A0 + lane, B0 + y, ("reduced", B0 + y, lane)) for lane in range(mA)]
 
 
-def item_pairs(mI, mJ, group_form):
+def item_pairs(mI, mJ):
     """Every warp step of an item: slots [0, mI) and, for a chunk pair, [mI, mI + mJ)."""
     Ms = mI + mJ
     steps = []
@@ -62,7 +57,7 @@ def item_pairs(mI, mJ, group_form):
         if mJ == 0:
             steps += list(diagonal_steps(A0, mA))
         for B0 in range(A0 + 32 if mJ == 0 else mI, Ms, 32):
-            steps += list(cross_steps(A0, mA, B0, min(32, Ms - B0), group_form))
+            steps += list(cross_steps(A0, mA, B0, min(32, Ms - B0)))
     return steps
 
 
@@ -77,11 +72,10 @@ def tree_merge(mB, written):
     return val[:mB]
 
 
-@pytest.mark.parametrize("group_form", [True, False])
 @pytest.mark.parametrize("mI,mJ", [(m, 0) for m in range(2, 65)] + [(64, m) for m in range(1, 65, 3)])
-def test_every_pair_once_and_distinct_targets(mI, mJ, group_form):
+def test_every_pair_once_and_distinct_targets(mI, mJ):
     seen = Counter()
-    for step in item_pairs(mI, mJ, group_form):
+    for step in item_pairs(mI, mJ):
         targets = [t for _, _, t in step]
         assert len(targets) == len(set(targets))
         for a, b, t in step:
@@ -101,7 +95,7 @@ def test_every_pair_once_and_distinct_targets(mI, mJ, group_form):
 @pytest.mark.parametrize("mB", list(range(1, 32)))
 def test_copy_tree_sums_each_copy_into_its_partner(mA, mB):
     written = set()
-    for step in cross_steps(0, mA, 32, mB, True):
+    for step in cross_steps(0, mA, 32, mB):
         for _, _, t in step:
             if t[0] == "copy":
                 written.add(t[1])

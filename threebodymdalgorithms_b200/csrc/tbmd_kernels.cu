@@ -79,26 +79,6 @@ __device__ __forceinline__ V3<A> warp_sum3(V3<A> v)
     return {warp_sum(v.x), warp_sum(v.y), warp_sum(v.z)};
 }
 
-// Warp sum in the arithmetic type S (butterfly; every lane gets the total).
-__device__ __forceinline__ float shfl_xor_s(float v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
-__device__ __forceinline__ double shfl_xor_s(double v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
-template <class T>
-__device__ __forceinline__ Dual<T> shfl_xor_s(Dual<T> v, int m)
-{
-    return {shfl_xor_s(v.v, m), shfl_xor_s(v.d, m)};
-}
-template <class S>
-__device__ __forceinline__ V3<S> warp_sum3s(V3<S> v)
-{
-#pragma unroll
-    for (int m = 16; m > 0; m >>= 1) {
-        v.x = v.x + shfl_xor_s(v.x, m);
-        v.y = v.y + shfl_xor_s(v.y, m);
-        v.z = v.z + shfl_xor_s(v.z, m);
-    }
-    return v;
-}
-
 // Edge x_j - x_i: FP64 subtraction, then hi/lo split (see split); the tangent carries d_j - d_i.
 template <class S>
 __device__ __forceinline__ void edge(const Pos &p, int64_t j, double xi, double yi, double zi, double dxi, double dyi,
@@ -1116,15 +1096,13 @@ cudaError_t launch_neighbors(int64_t n, const Grid &g, const GridSet &set, const
 // lane x owns slot A+x: its edge and its gradient accumulator live in registers.
 //   - pairs inside A: circular diagonals, pair (x, (x + d) mod m_A), d = 1 .. m_A/2 (on the half
 //     diagonal of an even m_A only x < m_A/2);
-//   - pairs A x B with a later block B: a full B (the FP64 and adjoint forms: m_B >= 24) by a
-//     rotation, pair (x, (x + t) & 31), t = 0..31.  A short B in the mixed forces form: lanes in
-//     groups of m_B, lane j of each group meets (j + t) mod m_B at step t = 0..m_B-1; groups after
-//     the first add their partner shares to per-warp copies, summed into B's slots at the end.  In
-//     the other forms each slot of B in turn against all lanes (broadcast steps).
+//   - pairs A x B with a later block B: a full B by a rotation, pair (x, (x + t) & 31),
+//     t = 0..31.  A short B: lanes in groups of m_B, lane j of each group meets (j + t) mod m_B at
+//     step t = 0..m_B-1; groups after the first add their partner shares to per-warp copies, summed
+//     into B's slots at the end.
 // In every warp step the partner slots (and copies) are distinct, so partner gradients are added with
-// a plain shared-memory read-modify-write (one __syncwarp per step, no atomics); in the broadcast
-// steps the partner gradient is first summed over the warp.  The own-slot gradient stays in
-// registers.  At the end of an item each slot is flushed with one FP64 atomic.
+// a plain shared-memory read-modify-write (one __syncwarp per step, no atomics).  The own-slot
+// gradient stays in registers.  At the end of an item each slot is flushed with one FP64 atomic.
 //
 // Cutoff test of the third edge: the reference's periodic formula (structs.hpp:106-115) on the third
 // edge the triplet math uses (FP32 in the mixed form, FP64 in the FP64 forms), or, when no list
@@ -1195,6 +1173,24 @@ __device__ __forceinline__ Grad<double> grad_shfl_down<double>(const Grad<double
     // w is padding in the FP64 accumulators
     return Grad<double>{__shfl_down_sync(0xffffffffu, v.x, off), __shfl_down_sync(0xffffffffu, v.y, off),
                         __shfl_down_sync(0xffffffffu, v.z, off), 0.0};
+}
+// the dual forms' accumulators: three dual components
+template <class T>
+__device__ __forceinline__ void grad_merge(Grad<Dual<T>> &dst, const Grad<Dual<T>> &src)
+{
+    dst.x = dst.x + src.x;
+    dst.y = dst.y + src.y;
+    dst.z = dst.z + src.z;
+}
+template <class T>
+__device__ __forceinline__ Dual<T> shfl_down_s(Dual<T> v, int off)
+{
+    return {__shfl_down_sync(0xffffffffu, v.v, off), __shfl_down_sync(0xffffffffu, v.d, off)};
+}
+template <class T>
+__device__ __forceinline__ Grad<Dual<T>> grad_shfl_down(const Grad<Dual<T>> &v, int off)
+{
+    return Grad<Dual<T>>{shfl_down_s(v.x, off), shfl_down_s(v.y, off), shfl_down_s(v.z, off)};
 }
 template <class S>
 __device__ __forceinline__ void slot_add(Grad<S> &slot, V3<S> g)
@@ -1298,9 +1294,8 @@ constexpr int P3_COPIES = 32;
 
 // The mixed forces kernel keeps a slot's neighbour index in the unused w of its lo-edge record (the
 // bits of an int32 in a float), so that the P3_COPIES accumulators of the group form of short blocks
-// fit in the shared memory of 8 CTAs per SM.  The FP64 forces kernel, whose occupancy its registers
-// bound, keeps its index array and adds the copies.  The adjoint forms reduce the partner shares of a
-// short block over the warp (broadcast steps).
+// fit in the shared memory of 8 CTAs per SM.  The FP64 and dual forms, whose occupancy their
+// registers bound, keep their index array and add the copies.
 template <class S>
 struct IdxInLo {
     static constexpr bool value = false;
@@ -1310,30 +1305,16 @@ struct IdxInLo<float> {
     static constexpr bool value = true;
 };
 template <class S>
-struct GroupCopies {
-    static constexpr bool value = false;
-};
-template <>
-struct GroupCopies<float> {
-    static constexpr bool value = true;
-};
-template <>
-struct GroupCopies<double> {
-    static constexpr bool value = true;
-};
-
-template <class S>
 struct SlotLayout {
     // per-warp shared memory, [2 * P3_CHUNK] of each: edge hi + b (Slot4), edge lo (Slot4, mixed only),
-    // gradient accumulator (Grad), neighbour index (unless IdxInLo); then, if IdxInLo, P3_COPIES
-    // gradient accumulators
+    // gradient accumulator (Grad), neighbour index (unless IdxInLo); then P3_COPIES gradient
+    // accumulators
     static constexpr bool mixed = HasLo<S>::value;
     static constexpr int nlo = mixed ? 1 : 0;
-    static constexpr bool copies = GroupCopies<S>::value;
     static constexpr size_t bytes_per_slot =
         (1 + nlo) * sizeof(Slot4<S>) + sizeof(Grad<S>) + (IdxInLo<S>::value ? 0 : sizeof(int32_t));
     static constexpr size_t bytes_per_warp =
-        2 * P3_CHUNK * bytes_per_slot + (copies ? P3_COPIES * sizeof(Grad<S>) : 0);
+        2 * P3_CHUNK * bytes_per_slot + P3_COPIES * sizeof(Grad<S>);
 };
 
 
@@ -1343,7 +1324,7 @@ struct P3Warp {
     Slot4<S> *sl;  // lo edge (mixed)
     Grad<S> *gr;   // gradient accumulators
     int32_t *idx;  // neighbour indices (unless IdxInLo)
-    Grad<S> *cp;   // [P3_COPIES] partner accumulators of lane groups >= 1 (if IdxInLo)
+    Grad<S> *cp;   // [P3_COPIES] partner accumulators of lane groups >= 1
     __device__ __forceinline__ int32_t index(int i) const
     {
         if constexpr (IdxInLo<S>::value)
@@ -1427,38 +1408,6 @@ __device__ __forceinline__ void pgrad_add_copy(const P3Warp<S> &W, int i, const 
     Grad<S> g = W.copy(i);
     pgrad_add(g, pg);
     W.set_copy(i, g);
-}
-// partner shares of all lanes for one common partner slot, added by lane 0
-template <class S>
-__device__ __forceinline__ void pgrad_add_warp(const P3Warp<S> &W, int i, const PGrad<S> &pg, int lane)
-{
-    const V3<S> g = warp_sum3s(pg.g);
-    if (lane == 0) {
-        Grad<S> v = W.grad(i);
-        slot_add(v, g);
-        W.set_grad(i, v);
-    }
-}
-template <>
-__device__ __forceinline__ void pgrad_add_warp<float>(const P3Warp<float> &W, int i, const PGrad<float> &pg, int lane)
-{
-    V3<float> g = pg.w * pg.ngamma;
-    float beta = pg.beta;
-#pragma unroll
-    for (int m = 16; m > 0; m >>= 1) {
-        g.x += __shfl_xor_sync(0xffffffffu, g.x, m);
-        g.y += __shfl_xor_sync(0xffffffffu, g.y, m);
-        g.z += __shfl_xor_sync(0xffffffffu, g.z, m);
-        beta += __shfl_xor_sync(0xffffffffu, beta, m);
-    }
-    if (lane == 0) {
-        Grad<float> v = W.grad(i);
-        v.x += g.x;
-        v.y += g.y;
-        v.z += g.z;
-        v.w += beta;
-        W.set_grad(i, v);
-    }
 }
 
 // Third-edge cutoff decision for slots a (own) and b (partner) with third edge w (cww = w.w).
@@ -1546,8 +1495,8 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
     W.sl = W.sd + SL;
     W.gr = (Grad<S> *)(W.sl + (L::nlo ? SL : 0));
     W.idx = IdxInLo<S>::value ? nullptr : (int32_t *)(W.gr + SL);
-    W.cp = !L::copies ? nullptr : IdxInLo<S>::value ? W.gr + SL : (Grad<S> *)(W.idx + SL);
-    if constexpr (L::copies) W.set_copy(lane, grad_zero<S>());
+    W.cp = IdxInLo<S>::value ? W.gr + SL : (Grad<S> *)(W.idx + SL);
+    W.set_copy(lane, grad_zero<S>());
     __syncwarp();
 
     const S nu = constant<S>(nu_d), nu3 = constant<S>(-3.0 * nu_d), nu15 = constant<S>(15.0 * nu_d);
@@ -1684,10 +1633,9 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
                 // pairs A x B with every later block B (of the same chunk, or of the second chunk)
                 for (int B0 = (mJ == 0 ? A0 + 32 : mI); B0 < Ms; B0 += 32) {
                     const int mB = min(32, Ms - B0);
-                    // a full block: 32 steps of distinct partners.  A short block takes mB steps in
-                    // lane groups (the mixed form) or broadcast steps with a warp reduction of the
-                    // partner share (the others, for mB < 24, where that beats 32 partly idle steps)
-                    if (mB >= (L::copies ? 32 : 24)) {
+                    // a full block: 32 steps of distinct partners; a short block: mB steps in lane
+                    // groups
+                    if (mB == 32) {
                         for (int t = 0; t < 32; ++t) {
                             const int y = (lane + t) & 31;
                             const bool act = own && y < mB;
@@ -1696,7 +1644,7 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
                             if (act) pgrad_add_at(W, b, gb);
                             __syncwarp();
                         }
-                    } else if constexpr (L::copies) {
+                    } else {
                         // a short block: lanes form groups of mB, and lane j of group g meets partner
                         // (j + t) mod mB at step t, so the partners of one group are distinct.  Group 0
                         // adds to B's slots and group g >= 1 to copy (g - 1) mB + y.  Then lane l takes
@@ -1728,12 +1676,6 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
                             W.set_grad(B0 + lane, gl);
                         }
                         __syncwarp();
-                    } else {
-                        for (int y = 0; y < mB; ++y) {
-                            const int b = B0 + y;
-                            pgrad_add_warp(W, b, pair(own, b), lane);
-                            __syncwarp();
-                        }
                     }
                 }
                 // merge the own accumulator into its slot
@@ -1771,9 +1713,11 @@ __global__ void __maxnreg__((P3MaxReg<S, ENERGY>::value))
         __syncwarp();
     };
 
-    if constexpr (Traits<S>::dual) {
-        // the dual forms run both kinds of item through one call site, which lets the compiler inline
-        // the item (two call sites left it an out-of-line function with a large stack frame)
+    if constexpr (!std::is_same<S, float>::value) {
+        // Both kinds of item through one call site.  The dual forms need it to get the item body
+        // inlined (two call sites left it out of line, with a stack frame of 620-710 bytes); the FP64
+        // forces kernel gains 0.8% at C3 and C4 from it, and the mixed forces kernel loses 3.5%, so it
+        // keeps the two loops below.
         for (int kind = 0; kind < 2; ++kind) {
             const unsigned int lim = kind == 0 ? (unsigned int)n : min(*cb.long_count, (unsigned int)cb.long_cap);
             unsigned int w = 0;
