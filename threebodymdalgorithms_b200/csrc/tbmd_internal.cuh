@@ -337,6 +337,7 @@ constexpr int P3_CHUNK = 64;
 
 struct CellBufs {
     int32_t *cell_of;      // [n] cell of each particle (input order)
+    int32_t *cell_rank;    // [n] its slot within the cell (the step's fused cell build)
     int32_t *cell_count;   // [ncells]
     int32_t *cell_start;   // [ncells + 1]
     int32_t *cell_fill;    // [ncells]

@@ -682,15 +682,17 @@ cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, const GridSet &
 }
 
 // The Simulation step of one system fuses the integrator into the cell build and the unsort:
-//   k_predict_assign  predictor (structs.hpp:40-55) and the cell of the moved particle
-//   k_scatter_gather  slot in the counting sort, and the particle's positions written to that slot
+//   k_predict_assign  predictor (structs.hpp:40-55), the cell of the moved particle and its rank in
+//                     the cell (the old count its atomic increment returns)
+//   k_scatter_gather  slot in the counting sort (cell start + rank), and the particle's positions
+//                     written to that slot
 //   k_update_record   update (structs.hpp:57-99) and the step's count record, after k_unsort
 // The arithmetic per particle is that of k_predictor / k_cell_assign / k_gather / k_update, so the
 // results are identical; the step needs fewer launches and passes over memory.
 __global__ void k_predict_assign(int64_t n, double *x, double *y, double *z, const double *vx, const double *vy,
                                  const double *vz, const double *ax, double dt, const __grid_constant__ Grid g,
-                                 int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count,
-                                 int32_t *__restrict__ cell_out)
+                                 int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_rank,
+                                 int32_t *__restrict__ cell_count, int32_t *__restrict__ cell_out)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -708,12 +710,12 @@ __global__ void k_predict_assign(int64_t n, double *x, double *y, double *z, con
     const int cz = cell_coord_w(pz, g.lo[2], g.w[2], g.dims[2], out);
     const int c = (int)TBMD_IX((cz * g.dims[1] + cy) * g.dims[0] + cx, g.ncells, BS_CELL_OF);
     cell_of[i] = c;
-    atomicAdd(cell_count + c, 1);
+    cell_rank[i] = atomicAdd(cell_count + c, 1);  // the particle's slot within its cell
     if (out) cell_out[c] = 1;
 }
 
 __global__ void k_scatter_gather(int64_t n, const int32_t *__restrict__ cell_of, const int32_t *__restrict__ start,
-                                 int32_t *__restrict__ fill, int32_t *__restrict__ sorted,
+                                 const int32_t *__restrict__ cell_rank, int32_t *__restrict__ sorted,
                                  const double *__restrict__ x, const double *__restrict__ y,
                                  const double *__restrict__ z, const __grid_constant__ Grid g, double *xs, double *ys,
                                  double *zs, float4 *qhi, float4 *qlo)
@@ -721,7 +723,7 @@ __global__ void k_scatter_gather(int64_t n, const int32_t *__restrict__ cell_of,
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int c = cell_of[i];
-    const int slot = (int)TBMD_IX(start[c] + atomicAdd(fill + c, 1), n, BS_CELL_SLOT);
+    const int slot = (int)TBMD_IX(start[c] + cell_rank[i], n, BS_CELL_SLOT);
     sorted[slot] = (int32_t)i;
     const double px = x[i], py = y[i], pz = z[i];
     xs[slot] = px;
@@ -774,9 +776,9 @@ cudaError_t launch_step_cells(int64_t n, double *const st13[13], double dt, cons
     cudaError_t e;
     if ((e = cudaMemsetAsync(cb.cell_count, 0, sizeof(int32_t) * 3 * g.ncells, st)) != cudaSuccess) return e;
     k_predict_assign<<<nb, 256, 0, st>>>(n, st13[0], st13[1], st13[2], st13[3], st13[4], st13[5], st13[6], dt, g,
-                                          cb.cell_of, cb.cell_count, cb.cell_out);
+                                          cb.cell_of, cb.cell_rank, cb.cell_count, cb.cell_out);
     k_cell_scan<<<1, 1024, 0, st>>>(g.ncells, cb.cell_count, cb.cell_start);
-    k_scatter_gather<<<nb, 256, 0, st>>>(n, cb.cell_of, cb.cell_start, cb.cell_fill, cb.sorted, st13[0], st13[1],
+    k_scatter_gather<<<nb, 256, 0, st>>>(n, cb.cell_of, cb.cell_start, cb.cell_rank, cb.sorted, st13[0], st13[1],
                                           st13[2], g, cb.xs, cb.ys, cb.zs, cb.qhi, cb.qlo);
     if (launches) *launches += 3;
     return cudaGetLastError();
@@ -944,7 +946,10 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(int64_t n, const _
             };
             if (staged && raw) {
                 // every coordinate lies in the box: the hi parts alone are within 2^-24 L, and the
-                // periodic form is the raw distance (each axis under 2 cells <= L / 2)
+                // periodic form is the raw distance (each axis under 2 cells <= L / 2).  Two
+                // iterations per trip let the next candidate's loads and test overlap this one's
+                // compaction (1% faster than one).
+#pragma unroll 2
                 for (int q0 = sl + 1; q0 < T; q0 += 32) {
                     const int q = q0 + lane;
                     const float4 h = shi[q];
@@ -956,6 +961,7 @@ __global__ void __launch_bounds__(NB_THREADS, 10) k_neighbors(int64_t n, const _
                     emit(pass, t);
                 }
             } else if (staged) {
+#pragma unroll 2
                 for (int q0 = sl + 1; q0 < T; q0 += 32) {
                     const int q = q0 + lane;
                     const float4 h = shi[q], l = slo[q];
