@@ -346,7 +346,7 @@ static tbmd_status ensure_cell_bufs(tbmd_ctx *ctx, int64_t n, int64_t nc, bool d
         // per particle: float4 qhi qlo; FP64 xs ys zs dxs dys dzs fs[3] hs[3]; int32 cell_of, sorted,
         // nbr_count, cell_rank
         CK(ctx->cell_n.ensure((size_t)n * (2 * sizeof(float4) + 12 * sizeof(double) + 4 * sizeof(int32_t)) + 256));
-        CK(ctx->cell_c.ensure((size_t)(4 * nc + 1) * sizeof(int32_t) + 256));
+        CK(ctx->cell_c.ensure((size_t)(3 * nc + 1) * sizeof(int32_t) + 256));
         CellBufs &cb = ctx->cb;
         cb.qhi = ctx->cell_n.as<float4>();
         cb.qlo = cb.qhi + n;
@@ -367,10 +367,9 @@ static tbmd_status ensure_cell_bufs(tbmd_ctx *ctx, int64_t n, int64_t nc, bool d
         cb.nbr_count = q + 2 * n;
         cb.cell_rank = q + 3 * n;
         int32_t *r = ctx->cell_c.as<int32_t>();
-        cb.cell_count = r;  // count, fill, out: adjacent (zeroed by one memset)
-        cb.cell_fill = r + nc;
-        cb.cell_out = r + 2 * nc;
-        cb.cell_start = r + 3 * nc;
+        cb.cell_count = r;  // count, out: adjacent (zeroed by one memset)
+        cb.cell_out = r + nc;
+        cb.cell_start = r + 2 * nc;
         ctx->cell_bufs_n = n;
         ctx->cell_bufs_cells = nc;
     }

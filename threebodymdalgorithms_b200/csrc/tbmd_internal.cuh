@@ -337,12 +337,11 @@ constexpr int P3_CHUNK = 64;
 
 struct CellBufs {
     int32_t *cell_of;      // [n] cell of each particle (input order)
-    int32_t *cell_rank;    // [n] its slot within the cell (the step's fused cell build)
+    int32_t *cell_rank;    // [n] its slot within the cell (the old count its increment returned)
     int32_t *cell_count;   // [ncells]
     int32_t *cell_start;   // [ncells + 1]
-    int32_t *cell_fill;    // [ncells]
     int32_t *cell_out;     // [ncells] 1 if the cell holds a particle whose raw coordinates lie outside the
-                           //          box (binned by wrapping); follows cell_fill in memory
+                           //          box (binned by wrapping); follows cell_count in memory
     int32_t *sorted;       // [n] sorted slot -> original index
     double *xs, *ys, *zs;  // [n] positions in sorted order
     float4 *qhi, *qlo;     // [n] sorted positions relative to the system's box corner lo, as FP32

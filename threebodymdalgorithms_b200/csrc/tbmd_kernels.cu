@@ -540,8 +540,8 @@ __device__ __forceinline__ int system_of(const int64_t *sys_off, int nsys, int64
 
 __global__ void k_cell_assign(int64_t n, const double *__restrict__ x, const double *__restrict__ y,
                               const double *__restrict__ z, const __grid_constant__ Grid g, GridSet set,
-                              int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count,
-                              int32_t *__restrict__ cell_out)
+                              int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_rank,
+                              int32_t *__restrict__ cell_count, int32_t *__restrict__ cell_out)
 {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -554,7 +554,7 @@ __global__ void k_cell_assign(int64_t n, const double *__restrict__ x, const dou
     int c = (int)(set.nsys > 1 ? set.cell_off[sys] : 0) + (cz * G.dims[1] + cy) * G.dims[0] + cx;
     c = (int)TBMD_IX(c, g.ncells, BS_CELL_OF);
     cell_of[i] = c;
-    atomicAdd(cell_count + c, 1);
+    cell_rank[i] = atomicAdd(cell_count + c, 1);  // the particle's slot within its cell
     if (out) cell_out[c] = 1;
 }
 
@@ -627,13 +627,11 @@ __global__ void __launch_bounds__(1024) k_cell_scan(int64_t ncells, const int32_
 }
 
 __global__ void k_cell_scatter(int64_t n, const int32_t *__restrict__ cell_of, const int32_t *__restrict__ start,
-                               int32_t *__restrict__ fill, int32_t *__restrict__ sorted)
+                               const int32_t *__restrict__ cell_rank, int32_t *__restrict__ sorted)
 {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    int c = cell_of[i];
-    int slot = atomicAdd(fill + c, 1);
-    sorted[TBMD_IX(start[c] + slot, n, BS_CELL_SLOT)] = (int32_t)i;
+    sorted[TBMD_IX(start[cell_of[i]] + cell_rank[i], n, BS_CELL_SLOT)] = (int32_t)i;
 }
 
 // Positions (and the adjoint direction) in sorted order, plus the FP32 hi/lo copy relative to the
@@ -670,11 +668,12 @@ cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, const GridSet &
 {
     const unsigned nb = (unsigned)((n + 255) / 256);
     cudaError_t e;
-    // cell_count, cell_fill and cell_out are adjacent: one memset
-    if ((e = cudaMemsetAsync(cb.cell_count, 0, sizeof(int32_t) * 3 * g.ncells, st)) != cudaSuccess) return e;
-    k_cell_assign<<<nb, 256, 0, st>>>(n, pos.x, pos.y, pos.z, g, set, cb.cell_of, cb.cell_count, cb.cell_out);
+    // cell_count and cell_out are adjacent: one memset
+    if ((e = cudaMemsetAsync(cb.cell_count, 0, sizeof(int32_t) * 2 * g.ncells, st)) != cudaSuccess) return e;
+    k_cell_assign<<<nb, 256, 0, st>>>(n, pos.x, pos.y, pos.z, g, set, cb.cell_of, cb.cell_rank, cb.cell_count,
+                                      cb.cell_out);
     k_cell_scan<<<1, 1024, 0, st>>>(g.ncells, cb.cell_count, cb.cell_start);
-    k_cell_scatter<<<nb, 256, 0, st>>>(n, cb.cell_of, cb.cell_start, cb.cell_fill, cb.sorted);
+    k_cell_scatter<<<nb, 256, 0, st>>>(n, cb.cell_of, cb.cell_start, cb.cell_rank, cb.sorted);
     k_gather<<<nb, 256, 0, st>>>(n, cb.sorted, pos, g, set, cb.xs, cb.ys, cb.zs, cb.qhi, cb.qlo,
                                  with_dir ? cb.dxs : nullptr, with_dir ? cb.dys : nullptr, with_dir ? cb.dzs : nullptr);
     if (launches) *launches += 4;
@@ -774,7 +773,7 @@ cudaError_t launch_step_cells(int64_t n, double *const st13[13], double dt, cons
 {
     const unsigned nb = (unsigned)((n + 255) / 256);
     cudaError_t e;
-    if ((e = cudaMemsetAsync(cb.cell_count, 0, sizeof(int32_t) * 3 * g.ncells, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(cb.cell_count, 0, sizeof(int32_t) * 2 * g.ncells, st)) != cudaSuccess) return e;
     k_predict_assign<<<nb, 256, 0, st>>>(n, st13[0], st13[1], st13[2], st13[3], st13[4], st13[5], st13[6], dt, g,
                                           cb.cell_of, cb.cell_rank, cb.cell_count, cb.cell_out);
     k_cell_scan<<<1, 1024, 0, st>>>(g.ncells, cb.cell_count, cb.cell_start);
