@@ -538,7 +538,7 @@ static tbmd_status enqueue_step(tbmd_ctx *ctx, cudaStream_t st, int *nl)
         phase_mark(ctx, st, PH_UPDATE, *nl);
         CK(launch_unsort_update(n, cb, s, ctx->cfg.dt, ctx->cfg.g, count_ptr(ctx),
                                 ctx->step_counts.as<unsigned long long>(), step_ptr(ctx), st));
-        *nl += 2;
+        *nl += 1;
         phase_mark(ctx, st, PH_END, *nl);
         return TBMD_OK;
     }

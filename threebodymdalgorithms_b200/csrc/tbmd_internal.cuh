@@ -337,7 +337,8 @@ constexpr int P3_CHUNK = 64;
 
 struct CellBufs {
     int32_t *cell_of;      // [n] cell of each particle (input order)
-    int32_t *cell_rank;    // [n] its slot within the cell (the old count its increment returned)
+    int32_t *cell_rank;    // [n] its rank within the cell (the old count its increment returned); the
+                           //     step's scatter replaces it by the particle's sorted slot
     int32_t *cell_count;   // [ncells]
     int32_t *cell_start;   // [ncells + 1]
     int32_t *cell_out;     // [ncells] 1 if the cell holds a particle whose raw coordinates lie outside the

@@ -685,7 +685,8 @@ cudaError_t launch_cell_build(int64_t n, Pos pos, const Grid &g, const GridSet &
 //                     the cell (the old count its atomic increment returns)
 //   k_scatter_gather  slot in the counting sort (cell start + rank), and the particle's positions
 //                     written to that slot
-//   k_update_record   update (structs.hpp:57-99) and the step's count record, after k_unsort
+//   k_update_record   unsort (a gather of the particle's force from its sorted slot), update
+//                     (structs.hpp:57-99) and the step's count record
 // The arithmetic per particle is that of k_predictor / k_cell_assign / k_gather / k_update, so the
 // results are identical; the step needs fewer launches and passes over memory.
 __global__ void k_predict_assign(int64_t n, double *x, double *y, double *z, const double *vx, const double *vy,
@@ -714,7 +715,7 @@ __global__ void k_predict_assign(int64_t n, double *x, double *y, double *z, con
 }
 
 __global__ void k_scatter_gather(int64_t n, const int32_t *__restrict__ cell_of, const int32_t *__restrict__ start,
-                                 const int32_t *__restrict__ cell_rank, int32_t *__restrict__ sorted,
+                                 int32_t *__restrict__ cell_rank, int32_t *__restrict__ sorted,
                                  const double *__restrict__ x, const double *__restrict__ y,
                                  const double *__restrict__ z, const __grid_constant__ Grid g, double *xs, double *ys,
                                  double *zs, float4 *qhi, float4 *qlo)
@@ -724,6 +725,7 @@ __global__ void k_scatter_gather(int64_t n, const int32_t *__restrict__ cell_of,
     const int c = cell_of[i];
     const int slot = (int)TBMD_IX(start[c] + cell_rank[i], n, BS_CELL_SLOT);
     sorted[slot] = (int32_t)i;
+    cell_rank[i] = slot;  // from here on the particle's sorted slot, for the update's force gather
     const double px = x[i], py = y[i], pz = z[i];
     xs[slot] = px;
     ys[slot] = py;
@@ -740,12 +742,15 @@ __global__ void k_unsort(int64_t n, const int32_t *__restrict__ sorted, const do
                          const double *__restrict__ f1, const double *__restrict__ f2, double *o0, double *o1,
                          double *o2);
 
-// update (structs.hpp:57-99, in input order, coalesced) and the step's triplet count record
-__global__ void k_update_record(int64_t n, double *vx, double *vy, double *vz, double *ax, double *ay, double *az,
-                                const double *__restrict__ fx, const double *__restrict__ fy,
-                                const double *__restrict__ fz, const double *__restrict__ m, double dt, double gx,
-                                double gy, double gz, unsigned long long *cur, unsigned long long *per_step,
-                                unsigned int *step)
+// unsort, update (structs.hpp:57-99) and the step's triplet count record, in input order: particle i
+// gathers its force from its sorted slot (recorded by k_scatter_gather), stores it in the state's
+// force arrays and updates its velocity and acceleration, so every state array is read and written
+// coalesced and only the three force loads are scattered
+__global__ void k_update_record(int64_t n, const int32_t *__restrict__ slot_of, const double *__restrict__ f0,
+                                const double *__restrict__ f1, const double *__restrict__ f2, double *vx, double *vy,
+                                double *vz, double *ax, double *ay, double *az, double *fxo, double *fyo,
+                                double *fzo, const double *__restrict__ m, double dt, double gx, double gy, double gz,
+                                unsigned long long *cur, unsigned long long *per_step, unsigned int *step)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {  // the step's triplet count (the triplet kernel has finished)
@@ -755,11 +760,16 @@ __global__ void k_update_record(int64_t n, double *vx, double *vy, double *vz, d
         *cur = 0ull;
     }
     if (i >= n) return;
+    const int64_t slot = TBMD_IX(slot_of[i], n, BS_SORTED);
+    const double fx = f0[slot], fy = f1[slot], fz = f2[slot];
+    fxo[i] = fx;
+    fyo[i] = fy;
+    fzo[i] = fz;
     const double h = __dmul_rn(dt, 0.5);
     const double mi = m[i];
-    const double nx = __dsub_rn(gx, __ddiv_rn(fx[i], mi));
-    const double ny = __dsub_rn(gy, __ddiv_rn(fy[i], mi));
-    const double nz = __dsub_rn(gz, __ddiv_rn(fz[i], mi));
+    const double nx = __dsub_rn(gx, __ddiv_rn(fx, mi));
+    const double ny = __dsub_rn(gy, __ddiv_rn(fy, mi));
+    const double nz = __dsub_rn(gz, __ddiv_rn(fz, mi));
     vx[i] = __dadd_rn(vx[i], __dmul_rn(nx, h));
     vy[i] = __dadd_rn(vy[i], __dmul_rn(ny, h));
     vz[i] = __dadd_rn(vz[i], __dmul_rn(nz, h));
@@ -788,10 +798,9 @@ cudaError_t launch_unsort_update(int64_t n, const CellBufs &cb, double *const st
                                  cudaStream_t st)
 {
     const unsigned nb = (unsigned)((n + 255) / 256);
-    // the scatter back to input order stays its own pass: the update then reads all arrays coalesced
-    k_unsort<<<nb, 256, 0, st>>>(n, cb.sorted, cb.fs[0], cb.fs[1], cb.fs[2], st13[10], st13[11], st13[12]);
-    k_update_record<<<nb, 256, 0, st>>>(n, st13[3], st13[4], st13[5], st13[6], st13[7], st13[8], st13[10], st13[11],
-                                         st13[12], st13[9], dt, g3[0], g3[1], g3[2], cur, per_step, step);
+    k_update_record<<<nb, 256, 0, st>>>(n, cb.cell_rank, cb.fs[0], cb.fs[1], cb.fs[2], st13[3], st13[4], st13[5],
+                                         st13[6], st13[7], st13[8], st13[10], st13[11], st13[12], st13[9], dt, g3[0],
+                                         g3[1], g3[2], cur, per_step, step);
     return cudaGetLastError();
 }
 
