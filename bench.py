@@ -381,13 +381,17 @@ def run_ours(args, world, rank, local):
         saved_steps, args.steps = args.steps, ksteps
         tot_k, trip_k = e2e_time(e2e_ksteps)
         args.steps = saved_steps
+        # the device copies of one tbmd_step_host call: in, x y z vx vy vz ax m (ay and az, which no step
+        # reads, stay on the host, where they are checked); out, x..az and fx fy fz (masses and IDs are
+        # copied on the host)
+        h2d, d2h = 8 * 8 * n, 12 * 8 * n
         e2e = {"value": e2e_all / (tot * 1e-3), "unit": "triplets/s", "ms_per_step": tot / args.steps,
-               "h2d_bytes_per_step": 10 * 8 * n + 4 * n, "d2h_bytes_per_step": 13 * 8 * n + 4 * n,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "path": "tbmd_step_host (state in, step, state out in one C-ABI call), pinned host SoA blocks",
                "separate_calls_ms_per_step": tot_sep / args.steps,
                "k_steps": {"k": KSTEPS, "calls": ksteps, "ms_per_step": tot_k / (ksteps * KSTEPS),
                            "value": trip_k / (tot_k * 1e-3), "unit": "triplets/s",
-                           "h2d_bytes_per_call": 10 * 8 * n + 4 * n, "d2h_bytes_per_call": 13 * 8 * n + 4 * n,
+                           "h2d_bytes_per_call": h2d, "d2h_bytes_per_call": d2h,
                            "path": "tbmd_step_host with K steps per call (state in, K steps, state out)"}}
         ctx.close()
 

@@ -137,7 +137,9 @@ tbmd_status tbmd_step(tbmd_ctx *ctx, int32_t iterations, uint64_t *triplets_per_
  * overlap one another.  The results are those of the three calls.  What differs is the overlap:
  * the last step's positions are final once its predictor has run and are copied back while its
  * forces are computed, masses (which no step changes) and IDs are copied on the host meanwhile,
- * and the whole call waits on the device once per attempt instead of once per call. */
+ * and the whole call waits on the device once per attempt instead of once per call.  With
+ * iterations > 0, ay and az are checked on the host but not copied to the device: a step reads ax
+ * alone (the predictor applies it on all three axes) and the update overwrites all three. */
 tbmd_status tbmd_step_host(tbmd_ctx *ctx, int64_t n, const int32_t *id, const double *x, const double *y,
                            const double *z, const double *vx, const double *vy, const double *vz, const double *ax,
                            const double *ay, const double *az, const double *m, int32_t iterations,

@@ -127,3 +127,31 @@ def test_contiguous_field_blocks():
     for k in KEYS:
         assert rel(back[k], ref[k]) <= 1e-12, k
     ctx.close()
+
+
+def test_step_host_leaves_the_unused_accelerations_out():
+    """A step reads ax alone (the predictor applies it on all three axes) and the update overwrites
+    ay and az, so tbmd_step_host does not copy them to the device.  The results are still those of
+    the three calls, and non-finite values there are still rejected, as tbmd_set_particles rejects
+    them."""
+    from threebodymdalgorithms_b200 import TbmdError
+    st = uniform_input("p3bca")
+    rng = np.random.default_rng(5)
+    st["ay"] = rng.normal(size=len(st["x"]))
+    st["az"] = rng.normal(size=len(st["x"]))
+    ref, cref = separate("p3bca", "fp64", 2.0, st, 1)
+    ctx = Context("p3bca", "fp64", 2.0, 0.001, G)
+    got, c = ctx.step_host(st, 1)
+    check_same(ref, cref, got, c, 1, "fp64")
+    for k, arr, bad in (("ay", 7, np.nan), ("az", 8, np.inf)):
+        b = {kk: np.array(v, copy=True) for kk, v in st.items()}
+        b[k][17] = bad
+        for call in (lambda: ctx.step_host(b, 1), lambda: ctx.set_state(b)):
+            with pytest.raises(TbmdError) as e:
+                call()
+            assert e.value.status == 2 and f"array {arr}" in str(e.value), str(e.value)
+    # the failed calls left the state of the good one
+    after = ctx.get_state()
+    for key in ("x", "vx", "ay", "fx"):
+        assert np.array_equal(after[key], got[key]), key
+    ctx.close()

@@ -716,8 +716,9 @@ uint64_t tbmd_kernel_launches(const tbmd_ctx *ctx) { return ctx ? ctx->launches 
 
 // The incoming particle arrays are in ctx->staging (x y z vx vy vz ax ay az m, n each): check them on
 // the device (non-finite values, masses <= 0, extremes of x, y, z for the domain) and make them the
-// context's state.  The state is untouched when the check fails.
-static tbmd_status commit_staging(tbmd_ctx *ctx, int64_t n, const int32_t *id)
+// context's state.  The state is untouched when the check fails.  host_bad flags arrays that the
+// caller checked on the host instead (bit k: array k holds a non-finite value).
+static tbmd_status commit_staging(tbmd_ctx *ctx, int64_t n, const int32_t *id, unsigned int host_bad = 0)
 {
     const size_t arr_bytes = sizeof(double) * 10 * (size_t)n;
     double *stg = ctx->staging.as<double>();
@@ -729,6 +730,7 @@ static tbmd_status commit_staging(tbmd_ctx *ctx, int64_t n, const int32_t *id)
     ValidateResult h{};
     CK(cudaMemcpyAsync(&h, vr, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));  // the caller's arrays are free again from here
+    h.bad_arrays |= host_bad;
     if (h.bad_arrays) {
         int k = 0;
         while (!(h.bad_arrays & (1u << k))) ++k;
@@ -766,13 +768,15 @@ static cudaError_t ensure_staging(tbmd_ctx *ctx, int64_t n)
     return ctx->staging.ensure(sizeof(double) * 10 * (size_t)n + sizeof(ValidateResult) + 256);
 }
 
-tbmd_status tbmd_set_particles(tbmd_ctx *ctx, int64_t n, const int32_t *id, const double *x, const double *y,
-                               const double *z, const double *vx, const double *vy, const double *vz,
-                               const double *ax, const double *ay, const double *az, const double *m)
+// tbmd_set_particles, and the input half of tbmd_step_host.  With `step_follows` the arrays ay and az
+// are not copied: a step reads ax alone (the predictor applies ax on all three axes,
+// structs.hpp:40-55) and the update overwrites all three, so their values cannot reach any result.
+// They are still checked, on the host while the other arrays travel, so the call fails on the same
+// inputs as tbmd_set_particles; the state holds zeros there until the first step.
+static tbmd_status upload_particles(tbmd_ctx *ctx, int64_t n, const int32_t *id, const double *const src[10],
+                                    bool step_follows)
 {
-    if (!ctx) return TBMD_INVALID_ARG;
     if (n < 1 || n > (int64_t)INT32_MAX / 2) return fail(ctx, TBMD_INVALID_ARG, "n = %lld out of range", (long long)n);
-    const double *src[10] = {x, y, z, vx, vy, vz, ax, ay, az, m};
     for (int k = 0; k < 10; ++k)
         if (!src[k]) return fail(ctx, TBMD_INVALID_ARG, "null particle array %d", k);
     tbmd_status st = check_device(ctx);
@@ -785,8 +789,29 @@ tbmd_status tbmd_set_particles(tbmd_ctx *ctx, int64_t n, const int32_t *id, cons
         dcol[k] = stg + (size_t)k * n;
         hcol[k] = const_cast<double *>(src[k]);
     }
-    CK(copy_columns(hcol, dcol, 0, 10, n, cudaMemcpyHostToDevice, ctx->stream));
-    return commit_staging(ctx, n, id);
+    unsigned int host_bad = 0;
+    if (step_follows) {
+        hcol[7] = hcol[8] = nullptr;  // copy_columns leaves null host entries out
+        CK(copy_columns(hcol, dcol, 0, 10, n, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemsetAsync(dcol[7], 0, sizeof(double) * 2 * (size_t)n, ctx->stream));  // ay, az adjacent
+        for (int k = 7; k <= 8; ++k) {
+            bool finite = true;
+            for (int64_t i = 0; i < n; ++i) finite &= std::isfinite(src[k][i]);
+            if (!finite) host_bad |= 1u << k;
+        }
+    } else {
+        CK(copy_columns(hcol, dcol, 0, 10, n, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    return commit_staging(ctx, n, id, host_bad);
+}
+
+tbmd_status tbmd_set_particles(tbmd_ctx *ctx, int64_t n, const int32_t *id, const double *x, const double *y,
+                               const double *z, const double *vx, const double *vy, const double *vz,
+                               const double *ax, const double *ay, const double *az, const double *m)
+{
+    if (!ctx) return TBMD_INVALID_ARG;
+    const double *src[10] = {x, y, z, vx, vy, vz, ax, ay, az, m};
+    return upload_particles(ctx, n, id, src, false);
 }
 
 void tbmd_generator_init(tbmd_generator *g)
@@ -1076,7 +1101,8 @@ tbmd_status tbmd_step_host(tbmd_ctx *ctx, int64_t n, const int32_t *id, const do
         CK(cudaEventCreateWithFlags(&ctx->pos_event, cudaEventDisableTiming));
         invalidate_graph(ctx);  // the step graph gains the position event
     }
-    st = tbmd_set_particles(ctx, n, id, x, y, z, vx, vy, vz, ax, ay, az, m);
+    const double *src[10] = {x, y, z, vx, vy, vz, ax, ay, az, m};
+    st = upload_particles(ctx, n, id, src, iterations > 0);
     if (st != TBMD_OK) return st;
     HostOut ho{{x_out, y_out, z_out, vx_out, vy_out, vz_out, ax_out, ay_out, az_out, m_out, fx_out, fy_out, fz_out}};
     // masses (no step changes them) and IDs come from the inputs, on the host, while the GPU works

@@ -2010,6 +2010,10 @@ __device__ __forceinline__ unsigned long long order_key(double d)
 
 __global__ void __launch_bounds__(256) k_validate(int64_t n, const double *__restrict__ a, ValidateResult *res)
 {
+    // per warp, then per block (shared memory), then one set of atomics per block: the result's
+    // fields share one L2 slice, where same-address atomics from every warp serialise
+    __shared__ unsigned int s_bad[8];
+    __shared__ unsigned long long s_bm[8], s_mn[8][3], s_mx[8][3];
     unsigned int bad = 0;
     unsigned long long bad_mass = ~0ull;
     unsigned long long mn[3] = {~0ull, ~0ull, ~0ull}, mx[3] = {0ull, 0ull, 0ull};
@@ -2027,25 +2031,48 @@ __global__ void __launch_bounds__(256) k_validate(int64_t n, const double *__res
             if (k == 9 && !(v > 0.0) && (unsigned long long)i < bad_mass) bad_mass = (unsigned long long)i;
         }
     }
+    auto warp_reduce = [&]() {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
-        const unsigned long long bm = __shfl_xor_sync(0xffffffffu, bad_mass, o);
-        bad_mass = bm < bad_mass ? bm : bad_mass;
+        for (int o = 16; o > 0; o >>= 1) {
+            bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+            const unsigned long long bm = __shfl_xor_sync(0xffffffffu, bad_mass, o);
+            bad_mass = bm < bad_mass ? bm : bad_mass;
 #pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const unsigned long long lo = __shfl_xor_sync(0xffffffffu, mn[k], o);
+                const unsigned long long hi = __shfl_xor_sync(0xffffffffu, mx[k], o);
+                mn[k] = lo < mn[k] ? lo : mn[k];
+                mx[k] = hi > mx[k] ? hi : mx[k];
+            }
+        }
+    };
+    warp_reduce();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        s_bad[warp] = bad;
+        s_bm[warp] = bad_mass;
         for (int k = 0; k < 3; ++k) {
-            const unsigned long long lo = __shfl_xor_sync(0xffffffffu, mn[k], o);
-            const unsigned long long hi = __shfl_xor_sync(0xffffffffu, mx[k], o);
-            mn[k] = lo < mn[k] ? lo : mn[k];
-            mx[k] = hi > mx[k] ? hi : mx[k];
+            s_mn[warp][k] = mn[k];
+            s_mx[warp][k] = mx[k];
         }
     }
-    if ((threadIdx.x & 31) == 0) {
-        if (bad) atomicOr(&res->bad_arrays, bad);
-        if (bad_mass != ~0ull) atomicMin(&res->bad_mass, bad_mass);
+    __syncthreads();
+    if (warp == 0) {
+        const bool has = lane < (int)(blockDim.x >> 5);
+        bad = has ? s_bad[lane] : 0u;
+        bad_mass = has ? s_bm[lane] : ~0ull;
         for (int k = 0; k < 3; ++k) {
-            atomicMin(&res->min_key[k], mn[k]);
-            atomicMax(&res->max_key[k], mx[k]);
+            mn[k] = has ? s_mn[lane][k] : ~0ull;
+            mx[k] = has ? s_mx[lane][k] : 0ull;
+        }
+        warp_reduce();
+        if (lane == 0) {
+            if (bad) atomicOr(&res->bad_arrays, bad);
+            if (bad_mass != ~0ull) atomicMin(&res->bad_mass, bad_mass);
+            for (int k = 0; k < 3; ++k) {
+                atomicMin(&res->min_key[k], mn[k]);
+                atomicMax(&res->max_key[k], mx[k]);
+            }
         }
     }
 }
