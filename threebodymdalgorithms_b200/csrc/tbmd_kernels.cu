@@ -1464,15 +1464,17 @@ __device__ __forceinline__ bool cut_inside(const P3Warp<S> &W, const CellBufs &c
     return sqdist_periodic(cb.xs[ta], cb.ys[ta], cb.zs[ta], cb.xs[tb], cb.ys[tb], cb.zs[tb], g) <= g.sqcut;
 }
 
-// Register cap of the triplet kernel per form.  The mixed forces kernel fits in 64 registers (32
-// resident warps per SM at 4 warps per block); the others keep about what they need unconstrained.
+// Register cap of the triplet kernel per form.  The mixed forces kernel runs at 72 registers (28
+// resident warps per SM at 4 warps per block): with the short-block lane groups, 72 took C3 from 0.444
+// to 0.430 ms and C4 from 30.1 to 28.2 ms against 64 (32 warps), and 80 gave 0.437 ms.  The others
+// keep about what they need unconstrained.
 template <class S, bool ENERGY>
 struct P3MaxReg {
     static constexpr int value = 128;
 };
 template <>
 struct P3MaxReg<float, false> {
-    static constexpr int value = 64;
+    static constexpr int value = 72;
 };
 template <>
 struct P3MaxReg<float, true> {
