@@ -1308,8 +1308,8 @@ constexpr int P3_COPIES = 32;
 
 // The mixed forces kernel keeps a slot's neighbour index in the unused w of its lo-edge record (the
 // bits of an int32 in a float), so that the P3_COPIES accumulators of the group form of short blocks
-// fit in the shared memory of 8 CTAs per SM.  The FP64 and dual forms, whose occupancy their
-// registers bound, keep their index array and add the copies.
+// take no more shared memory than the index array did (26.6 KB per CTA of 4 warps).  The FP64 and
+// dual forms, whose occupancy their registers bound, keep their index array and add the copies.
 template <class S>
 struct IdxInLo {
     static constexpr bool value = false;
