@@ -189,12 +189,12 @@ def barrier(world):
 
 
 # Algorithmic bytes per particle of the P3BCA step's cell build (predictor fused in), each array
-# access counted once: k_predict_assign reads x, y, z, vx, vy, vz, ax (56 B), writes x, y, z (24 B)
-# and the cell index (4 B), and adds to the cell's count (8 B); k_scatter_gather reads the cell
-# index, its start and fill counter (16 B) and x, y, z (24 B), and writes the sorted index (4 B),
-# the sorted FP64 positions (24 B) and their FP32 hi/lo copies (32 B).  The scan over the cells
-# adds under 1 B per particle.
-CELL_BUILD_BYTES = 92 + 100
+# access counted once: k_predict_assign reads x, y, z, vx, vy, vz, ax (56 B), writes x, y, z (24 B),
+# the cell index and the rank in the cell (8 B), and adds to the cell's count (8 B);
+# k_scatter_gather reads the cell index, the rank and the cell's start (12 B) and x, y, z (24 B),
+# and writes the sorted index and the slot (8 B), the sorted FP64 positions (24 B) and their FP32
+# hi/lo copies (32 B).  The scan over the cells adds under 1 B per particle.
+CELL_BUILD_BYTES = 96 + 100
 
 
 def hbm_peak():
