@@ -513,6 +513,35 @@ def test_bad_inputs_are_rejected():
     ctx.close()
 
 
+def test_input_check_over_many_blocks():
+    """The input check reduces per warp, then per block, then across blocks: with 100,000 particles
+    the lowest bad array, the lowest non-positive mass and the domain extremes (as
+    RegularGridDecomposition::getDomainMinMax gives them, padded by 1e-4) must still come out exact."""
+    from threebodymdalgorithms_b200 import TbmdError
+    n = 100_000
+    st = generators.uniform(n, (40, 40, 40))
+    ctx = Context("p3bca", "fp64", 2.0)
+    ctx.set_state(st)
+    _, _, L, lo = ctx.cells(with_particles=False)
+    for d, k in enumerate(("x", "y", "z")):
+        a, b = st[k].min() - 0.0001, st[k].max() + 0.0001
+        assert lo[d] == a and L[d] == abs(b - a), k
+    bad = {k: np.array(v, copy=True) for k, v in st.items()}
+    bad["vz"][77_777] = np.inf  # array 5, in a late block
+    bad["y"][99_999] = np.nan   # array 1, in the last block
+    with pytest.raises(TbmdError) as e:
+        ctx.set_state(bad)
+    assert e.value.status == 2 and "array 1" in str(e.value), str(e.value)
+    bad = {k: np.array(v, copy=True) for k, v in st.items()}
+    bad["m"][93_000] = -1.0
+    bad["m"][1_234] = 0.0
+    bad["m"][50_001] = 0.0
+    with pytest.raises(TbmdError) as e:
+        ctx.set_state(bad)
+    assert e.value.status == 2 and "particle 1234 " in str(e.value), str(e.value)
+    ctx.close()
+
+
 def test_autotune_keeps_results(tmp_path):
     st = generators.uniform(2048, (12, 12, 12))
     ref, _, _ = forces_of("auta", "mixed", st)
