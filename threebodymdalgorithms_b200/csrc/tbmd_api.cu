@@ -4,6 +4,7 @@
 // replayed; per-step triplet counts are recorded on the device and read back once per call.
 #include <cuda_runtime.h>
 
+#include <cfloat>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -795,9 +796,11 @@ static tbmd_status upload_particles(tbmd_ctx *ctx, int64_t n, const int32_t *id,
         CK(copy_columns(hcol, dcol, 0, 10, n, cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaMemsetAsync(dcol[7], 0, sizeof(double) * 2 * (size_t)n, ctx->stream));  // ay, az adjacent
         for (int k = 7; k <= 8; ++k) {
-            bool finite = true;
-            for (int64_t i = 0; i < n; ++i) finite &= std::isfinite(src[k][i]);
-            if (!finite) host_bad |= 1u << k;
+            // branch-free, so the compiler vectorises it: |v| <= DBL_MAX is false for inf and NaN
+            const double *a = src[k];
+            int bad = 0;
+            for (int64_t i = 0; i < n; ++i) bad |= !(std::fabs(a[i]) <= DBL_MAX);
+            if (bad) host_bad |= 1u << k;
         }
     } else {
         CK(copy_columns(hcol, dcol, 0, 10, n, cudaMemcpyHostToDevice, ctx->stream));
